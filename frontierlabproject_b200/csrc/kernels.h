@@ -1,0 +1,31 @@
+// Kernel launchers of libqsim_b200 (all on the caller's stream).
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qsb {
+
+// pass kernel (kern_pass.cu)
+cudaError_t launch_pass_kernel(int dtype, const uint8_t* d_prog, void* psi, int pass_begin, int pass_end,
+                               int threads, size_t smem, int grid, bool cooperative, unsigned* bar,
+                               unsigned* err, uint64_t limit_ns, cudaStream_t stream);
+cudaError_t pass_kernel_occupancy(int dtype, int threads, size_t smem, int* blocks_per_sm);
+
+// per-gate kernels: one full sweep per gate (kern_gate.cu)
+cudaError_t launch_gate1(int dtype, void* psi, int n, int q, const std::complex<double>* U, cudaStream_t s);
+cudaError_t launch_gate2(int dtype, void* psi, int n, int q0, int q1, const std::complex<double>* U,
+                         cudaStream_t s);
+cudaError_t launch_diag1(int dtype, void* psi, int n, int q, std::complex<double> d0, std::complex<double> d1,
+                         cudaStream_t s);
+// out[j] = in[i], j = sum_p bit_p(i) << map[p]   (out-of-place)
+cudaError_t launch_permute_scatter(int dtype, const void* in, void* out, int n, const int* map, cudaStream_t s);
+
+// reductions into double accumulators (kern_gate.cu); acc must be zeroed by the caller
+cudaError_t launch_norm2(int dtype, const void* psi, int n, double* acc, cudaStream_t s);
+cudaError_t launch_inner(int dtype, const void* a, const void* b, int n, double* acc2, cudaStream_t s);
+cudaError_t launch_set_basis(int dtype, void* psi, int n, uint64_t index, cudaStream_t s);
+
+int device_sm_count();
+
+}  // namespace qsb

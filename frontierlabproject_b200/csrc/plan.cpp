@@ -1,0 +1,547 @@
+// Pass / phase planning and program encoding for the pass kernel.
+#include "plan.h"
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+
+namespace qsb {
+
+static inline uint64_t bit(int p) { return 1ull << p; }
+static inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+static bool is_zero(const cplx& z) { return z.real() == 0.0 && z.imag() == 0.0; }
+static bool is_one(const cplx& z) { return z.real() == 1.0 && z.imag() == 0.0; }
+
+COp classify(const QOp& op) {
+  COp c;
+  const cplx* U = op.U;
+  if (op.arity == 1) {
+    c.a = op.q0;
+    c.touch = bit(op.q0);
+    if (is_zero(U[1]) && is_zero(U[2])) {
+      c.kind = GK_1Q_DIAG; c.ncoef = 2; c.coef[0] = U[0]; c.coef[1] = U[3];
+      c.need = 0;
+      return c;
+    }
+    c.need = bit(op.q0);
+    if (is_zero(U[0]) && is_zero(U[3]) && is_one(U[1]) && is_one(U[2])) {
+      c.kind = GK_1Q_X; c.ncoef = 0;
+      return c;
+    }
+    c.ncoef = 4;
+    for (int i = 0; i < 4; ++i) c.coef[i] = U[i];
+    bool real = true, reim = true;
+    for (int i = 0; i < 4; ++i) if (U[i].imag() != 0.0) real = false;
+    if (U[0].imag() != 0.0 || U[3].imag() != 0.0 || U[1].real() != 0.0 || U[2].real() != 0.0) reim = false;
+    c.kind = real ? GK_1Q_REAL : (reim ? GK_1Q_REIM : GK_1Q_DENSE);
+    return c;
+  }
+  // two-qubit; index = b_q0 + 2 b_q1
+  const int q0 = op.q0, q1 = op.q1;
+  c.touch = bit(q0) | bit(q1);
+  auto M = [&](int r, int col) { return U[4 * r + col]; };
+  bool diag = true;
+  for (int r = 0; r < 4; ++r)
+    for (int col = 0; col < 4; ++col)
+      if (r != col && !is_zero(M(r, col))) diag = false;
+  if (diag) {
+    c.kind = GK_2Q_DIAG; c.a = q0; c.b = q1; c.ncoef = 4;
+    for (int i = 0; i < 4; ++i) c.coef[i] = M(i, i);
+    c.need = 0;
+    return c;
+  }
+  // SWAP
+  {
+    static const int P[4] = {0, 2, 1, 3};
+    bool sw = true;
+    for (int r = 0; r < 4; ++r)
+      for (int col = 0; col < 4; ++col) {
+        cplx want = (col == P[r]) ? cplx(1, 0) : cplx(0, 0);
+        if (M(r, col) != want) sw = false;
+      }
+    if (sw) {
+      c.kind = GK_2Q_SWAP; c.a = q0; c.b = q1; c.ncoef = 0; c.need = c.touch;
+      return c;
+    }
+  }
+  // controlled on matrix bit cb (0 -> q0, 1 -> q1): identity where that bit is 0 and
+  // no coupling between the two halves.
+  for (int cb = 0; cb < 2; ++cb) {
+    const int cm = 1 << cb, tm = 1 << (1 - cb);
+    bool ok = true;
+    for (int r = 0; r < 4 && ok; ++r)
+      for (int col = 0; col < 4 && ok; ++col) {
+        const bool rc = r & cm, cc = col & cm;
+        if (!rc || !cc) {
+          cplx want = (r == col && !rc) ? cplx(1, 0) : cplx(0, 0);
+          if (M(r, col) != want) ok = false;
+        }
+      }
+    if (!ok) continue;
+    // block on the control = 1 half: rows/cols cm and cm|tm
+    cplx u00 = M(cm, cm), u01 = M(cm, cm | tm), u10 = M(cm | tm, cm), u11 = M(cm | tm, cm | tm);
+    c.a = cb == 0 ? q0 : q1;
+    c.b = cb == 0 ? q1 : q0;
+    c.need = bit(c.b);
+    if (is_zero(u00) && is_zero(u11) && is_one(u01) && is_one(u10)) {
+      c.kind = GK_2Q_CX; c.ncoef = 0;
+    } else {
+      c.kind = GK_2Q_CU; c.ncoef = 4;
+      c.coef[0] = u00; c.coef[1] = u01; c.coef[2] = u10; c.coef[3] = u11;
+    }
+    return c;
+  }
+  c.kind = GK_2Q_DENSE; c.a = q0; c.b = q1; c.ncoef = 16;
+  for (int i = 0; i < 16; ++i) c.coef[i] = U[i];
+  c.need = c.touch;
+  return c;
+}
+
+// ---------------------------------------------------------------------------------
+// Greedy + hill-climbing choice of a bit set of size `cap` (containing `forced`) that
+// executes the longest dependency-closed run of the remaining ops.
+// ---------------------------------------------------------------------------------
+namespace {
+
+struct Scan {
+  const std::vector<COp>& ops;
+  uint64_t universe;   // bits whose blocking ends the scan
+  // ops (in order) executable with staged set S
+  void run(const std::vector<int>& rem, uint64_t S, std::vector<int>& out) const {
+    out.clear();
+    uint64_t blocked = 0;
+    for (int i : rem) {
+      const COp& o = ops[i];
+      if (o.touch & blocked) { blocked |= o.touch; }
+      else if ((o.need & ~S) == 0) { out.push_back(i); }
+      else { blocked |= o.touch; }
+      if ((blocked & universe) == universe) break;
+    }
+  }
+  size_t count(const std::vector<int>& rem, uint64_t S) const {
+    size_t c = 0;
+    uint64_t blocked = 0;
+    for (int i : rem) {
+      const COp& o = ops[i];
+      if (o.touch & blocked) { blocked |= o.touch; }
+      else if ((o.need & ~S) == 0) { ++c; }
+      else { blocked |= o.touch; }
+      if ((blocked & universe) == universe) break;
+    }
+    return c;
+  }
+};
+
+uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candidates, uint64_t forced,
+                    int cap, int iters) {
+  uint64_t S = forced;
+  // greedy seed in op order
+  uint64_t blocked = 0;
+  std::vector<uint64_t> lookahead;
+  for (int i : rem) {
+    const COp& o = sc.ops[i];
+    if (o.touch & blocked) { blocked |= o.touch; if (o.need) lookahead.push_back(o.need); continue; }
+    if ((o.need & ~S) == 0) continue;
+    if (popc(S | o.need) <= cap) S |= o.need;
+    else { blocked |= o.touch; lookahead.push_back(o.need); }
+    if ((blocked & sc.universe) == sc.universe) break;
+  }
+  // fill with bits the blocked ops need next, then the lowest free bits
+  for (uint64_t nd : lookahead) {
+    if (popc(S) >= cap) break;
+    if (popc(S | nd) <= cap) S |= nd;
+  }
+  for (int p = 0; p < 64 && popc(S) < cap; ++p)
+    if ((candidates & bit(p)) && !(S & bit(p))) S |= bit(p);
+  size_t best = sc.count(rem, S);
+  for (int it = 0; it < iters; ++it) {
+    bool improved = false;
+    for (int a = 0; a < 64 && !improved; ++a) {
+      if (!(S & bit(a)) || (forced & bit(a))) continue;
+      for (int b = 0; b < 64; ++b) {
+        if (!(candidates & bit(b)) || (S & bit(b))) continue;
+        uint64_t T = (S & ~bit(a)) | bit(b);
+        size_t c = sc.count(rem, T);
+        if (c > best) { best = c; S = T; improved = true; break; }
+      }
+    }
+    if (!improved) break;
+  }
+  return S;
+}
+
+std::vector<int> bits_of(uint64_t m) {
+  std::vector<int> v;
+  for (int p = 0; p < 64; ++p) if (m & bit(p)) v.push_back(p);
+  return v;
+}
+
+}  // namespace
+
+static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const std::vector<int>& pass_ops,
+                                             const std::vector<int>& sbits, int r, int iters) {
+  // Phases choose register bits among the staged physical bits; op need masks are
+  // physical, so the phase set is a physical mask, converted to local bits at the end.
+  uint64_t Smask = 0;
+  for (int p : sbits) Smask |= bit(p);
+  const int rr = std::min<int>(r, (int)sbits.size());
+  Scan sc{ops, Smask};
+  std::vector<PlannedPhase> phases;
+  std::vector<int> rem = pass_ops, taken, rest;
+  while (!rem.empty()) {
+    uint64_t R = choose_set(sc, rem, Smask, 0, rr, iters);
+    sc.run(rem, R, taken);
+    if (taken.empty()) throw std::runtime_error("planner: phase made no progress");
+    PlannedPhase ph;
+    for (int p : bits_of(R)) {
+      auto it = std::find(sbits.begin(), sbits.end(), p);
+      ph.rbits.push_back((int)(it - sbits.begin()));
+    }
+    ph.ops = taken;
+    phases.push_back(ph);
+    rest.clear();
+    size_t t = 0;
+    for (int i : rem) {
+      if (t < taken.size() && taken[t] == i) { ++t; continue; }
+      rest.push_back(i);
+    }
+    rem.swap(rest);
+  }
+  return phases;
+}
+
+std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const PlanConfig& cfg) {
+  std::vector<PlannedPass> out;
+  if (ops.empty()) return out;
+  const int m = std::min(cfg.m, n);
+  const int k = std::min(cfg.k, m);
+  const uint64_t all = (n >= 64) ? ~0ull : (bit(n) - 1);
+  const uint64_t forced = (k >= 64) ? ~0ull : (bit(k) - 1);
+  Scan sc{ops, all};
+  std::vector<int> rem(ops.size()), taken, rest;
+  for (size_t i = 0; i < ops.size(); ++i) rem[i] = (int)i;
+  while (!rem.empty()) {
+    uint64_t S = (m == n) ? all : choose_set(sc, rem, all, forced, m, cfg.hill_iters);
+    sc.run(rem, S, taken);
+    if (taken.empty()) throw std::runtime_error("planner: pass made no progress");
+    PlannedPass ps;
+    ps.sbits = bits_of(S);
+    ps.ops = taken;
+    ps.phases = plan_phases(ops, taken, ps.sbits, cfg.r, cfg.hill_iters);
+    out.push_back(std::move(ps));
+    rest.clear();
+    size_t t = 0;
+    for (int i : rem) {
+      if (t < taken.size() && taken[t] == i) { ++t; continue; }
+      rest.push_back(i);
+    }
+    rem.swap(rest);
+  }
+  return out;
+}
+
+std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, const PlanConfig& cfg) {
+  // perm[b] = destination bit of the data at bit b.  Cycles are packed into passes whose
+  // staged set (always holding the k lowest bits) has at most m bits; a cycle longer than
+  // the free room is split: (c0 .. cL-1) = (c0 c_{j+1} .. c_{L-1}) after (c0 .. c_j).
+  std::vector<PlannedPass> out;
+  const int m = std::min(cfg.m, n);
+  const int k = std::min(cfg.k, m);
+  std::vector<int> cur(n);
+  for (int b = 0; b < n; ++b) cur[b] = perm[b];
+  // pieces: each a list of positions (c0, c1, ..., c_{L-1}) meaning data at c_i -> c_{i+1}
+  std::vector<std::vector<int>> pieces;
+  std::vector<bool> seen(n, false);
+  for (int b = 0; b < n; ++b) {
+    if (seen[b] || cur[b] == b) { seen[b] = true; continue; }
+    std::vector<int> cyc;
+    int x = b;
+    while (!seen[x]) { seen[x] = true; cyc.push_back(x); x = cur[x]; }
+    pieces.push_back(cyc);
+  }
+  auto extra = [&](const std::vector<int>& c) {
+    int e = 0;
+    for (int p : c) if (p >= k) ++e;
+    return e;
+  };
+  const int room = m - k;
+  // split long cycles
+  std::vector<std::vector<int>> fitted;
+  for (auto& c : pieces) {
+    std::vector<int> cyc = c;
+    while (extra(cyc) > room) {
+      // take the longest prefix c0..cj with extra() <= room
+      std::vector<int> head;
+      for (size_t i = 0; i < cyc.size(); ++i) {
+        head.push_back(cyc[i]);
+        if (extra(head) > room) { head.pop_back(); break; }
+      }
+      if (head.size() < 2) throw std::runtime_error("planner: cannot split permutation cycle");
+      fitted.push_back(head);
+      std::vector<int> tail;
+      tail.push_back(cyc[0]);
+      for (size_t i = head.size(); i < cyc.size(); ++i) tail.push_back(cyc[i]);
+      cyc.swap(tail);
+    }
+    if (cyc.size() >= 2) fitted.push_back(cyc);
+  }
+  // pack pieces in order into passes (pieces of one cycle stay in order; a piece that
+  // shares a position with the open pass starts a new pass)
+  std::vector<std::vector<std::vector<int>>> groups;
+  std::vector<uint64_t> gmask;
+  for (auto& pc : fitted) {
+    uint64_t pm = 0;
+    for (int p : pc) pm |= bit(p);
+    bool placed = false;
+    if (!groups.empty()) {
+      uint64_t gm = gmask.back();
+      uint64_t hi = (gm | pm) & ~((k >= 64) ? ~0ull : (bit(k) - 1));
+      if (!(gm & pm) && popc(hi) <= room) {
+        groups.back().push_back(pc);
+        gmask.back() |= pm;
+        placed = true;
+      }
+    }
+    if (!placed) { groups.push_back({pc}); gmask.push_back(pm); }
+  }
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    uint64_t S = gmask[gi] | ((k >= 64) ? ~0ull : (bit(k) - 1));
+    // fill to m with the lowest free bits (keeps the group count at 2^(n-m))
+    for (int p = 0; p < n && popc(S) < m; ++p) S |= bit(p);
+    PlannedPass ps;
+    ps.sbits = bits_of(S);
+    std::vector<int> dest(n);
+    for (int b = 0; b < n; ++b) dest[b] = b;
+    for (auto& pc : groups[gi])
+      for (size_t i = 0; i < pc.size(); ++i) dest[pc[i]] = pc[(i + 1) % pc.size()];
+    ps.store_src.assign(ps.sbits.size(), 0);
+    for (size_t u = 0; u < ps.sbits.size(); ++u) {
+      int d = dest[ps.sbits[u]];
+      auto it = std::find(ps.sbits.begin(), ps.sbits.end(), d);
+      ps.store_src[it - ps.sbits.begin()] = (int)u;
+    }
+    out.push_back(std::move(ps));
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------------
+// Encoding
+// ---------------------------------------------------------------------------------
+static uint64_t fnv(uint64_t h, const void* p, size_t n) {
+  const uint8_t* b = (const uint8_t*)p;
+  for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+  return h;
+}
+
+// Thread-bit order: the first five (the lane bits) cover as many shared-memory bank
+// classes as possible, given the swizzle of the dtype.
+static std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype) {
+  auto cls = [&](int j) {
+    if (dtype == 0) return j == 0 ? 0 : 1 + (j - 1) % 3;
+    return j % 3;
+  };
+  std::vector<int> rest = tb, out;
+  std::vector<bool> covered(4, false);
+  for (int c = 0; c < 4 && out.size() < 5; ++c) {
+    for (size_t i = 0; i < rest.size(); ++i) {
+      int kc = cls(rest[i]);
+      if (!covered[kc]) {
+        covered[kc] = true;
+        out.push_back(rest[i]);
+        rest.erase(rest.begin() + i);
+        break;
+      }
+    }
+  }
+  std::sort(out.begin(), out.end());
+  while (out.size() < 5 && !rest.empty()) { out.push_back(rest.front()); rest.erase(rest.begin()); }
+  for (int j : rest) out.push_back(j);
+  return out;
+}
+
+Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops, int n,
+                       int dtype) {
+  Program prog;
+  std::vector<PassDesc> pd;
+  std::vector<PhaseDesc> phd;
+  std::vector<GateInstr> gi;
+  std::vector<cplx> coef;
+  int threads = 32;
+  size_t smem = 0;
+  const size_t esz = dtype == 0 ? 8 : 16;
+  for (const PlannedPass& ps : passes) {
+    PassDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.m = (int)ps.sbits.size();
+    // register bits per thread are fixed by the dtype (the kernel's template parameter);
+    // 2^(r - item bits) = 16 load/store items per thread
+    const int r = dtype == 0 ? 5 : 4;
+    if (d.m < r || d.m - r > 8) throw std::runtime_error("encoder: pass size outside the kernel's geometry");
+    d.r = r;
+    d.phase0 = (int)phd.size();
+    d.nphase = (int)ps.phases.size();
+    uint64_t S = 0;
+    for (int j = 0; j < d.m; ++j) { d.sbit[j] = (int8_t)ps.sbits[j]; S |= bit(ps.sbits[j]); }
+    int g = 0;
+    for (int p = 0; p < n; ++p) if (!(S & bit(p))) d.gbit[g++] = (int8_t)p;
+    d.ngbits = g;
+    d.store_perm = ps.store_src.empty() ? 0 : 1;
+    for (size_t j = 0; j < ps.store_src.size(); ++j) d.store_src[j] = (int8_t)ps.store_src[j];
+    threads = std::max(threads, 1 << (d.m - r));
+    smem = std::max(smem, (size_t)2 * (esz << d.m));  // two group buffers (double buffering)
+    for (const PlannedPhase& ph : ps.phases) {
+      PhaseDesc h;
+      std::memset(&h, 0, sizeof(h));
+      if ((int)ph.rbits.size() != r) throw std::runtime_error("encoder: register count differs within a pass");
+      std::vector<int> tb;
+      uint64_t Rl = 0;
+      for (int j = 0; j < r; ++j) { h.rbit[j] = (int8_t)ph.rbits[j]; Rl |= bit(ph.rbits[j]); }
+      for (int j = 0; j < d.m; ++j) if (!(Rl & bit(j))) tb.push_back(j);
+      tb = order_thread_bits(tb, dtype);
+      for (size_t j = 0; j < tb.size(); ++j) h.tbit[j] = (int8_t)tb[j];
+      h.gate0 = (int)gi.size();
+      h.ngate = (int)ph.ops.size();
+      // physical bit -> register index for this phase
+      int reg_of_phys[kMaxQubits];
+      for (int p = 0; p < kMaxQubits; ++p) reg_of_phys[p] = -1;
+      for (int j = 0; j < r; ++j) reg_of_phys[ps.sbits[ph.rbits[j]]] = j;
+      auto opnd = [&](int p) -> uint8_t {
+        return reg_of_phys[p] >= 0 ? (uint8_t)reg_of_phys[p] : (uint8_t)(kFixed + p);
+      };
+      for (int oi : ph.ops) {
+        const COp& o = ops[oi];
+        GateInstr g2;
+        std::memset(&g2, 0, sizeof(g2));
+        g2.kind = o.kind;
+        g2.a = opnd(o.a);
+        g2.b = o.b >= 0 ? opnd(o.b) : 0;
+        g2.coef = (int)coef.size();
+        for (int c = 0; c < o.ncoef; ++c) coef.push_back(o.coef[c]);
+        gi.push_back(g2);
+      }
+      phd.push_back(h);
+    }
+    pd.push_back(d);
+  }
+  ProgramHeader hdr;
+  std::memset(&hdr, 0, sizeof(hdr));
+  hdr.npass = (int)pd.size();
+  hdr.nphase = (int)phd.size();
+  hdr.ngate = (int)gi.size();
+  hdr.ncoef = (int)coef.size();
+  hdr.n = n;
+  hdr.dtype = dtype;
+  hdr.max_threads = threads;
+  auto align16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+  size_t off = align16(sizeof(hdr));
+  hdr.off_pass = (int)off; off = align16(off + pd.size() * sizeof(PassDesc));
+  hdr.off_phase = (int)off; off = align16(off + phd.size() * sizeof(PhaseDesc));
+  hdr.off_gate = (int)off; off = align16(off + gi.size() * sizeof(GateInstr));
+  hdr.off_coef = (int)off; off = align16(off + coef.size() * esz);
+  prog.bytes.assign(off, 0);
+  std::memcpy(prog.bytes.data(), &hdr, sizeof(hdr));
+  if (!pd.empty()) std::memcpy(prog.bytes.data() + hdr.off_pass, pd.data(), pd.size() * sizeof(PassDesc));
+  if (!phd.empty()) std::memcpy(prog.bytes.data() + hdr.off_phase, phd.data(), phd.size() * sizeof(PhaseDesc));
+  if (!gi.empty()) std::memcpy(prog.bytes.data() + hdr.off_gate, gi.data(), gi.size() * sizeof(GateInstr));
+  uint64_t h = 1469598103934665603ull;
+  h = fnv(h, prog.bytes.data(), hdr.off_coef);  // everything except coefficient values
+  if (dtype == 0) {
+    float* cf = (float*)(prog.bytes.data() + hdr.off_coef);
+    for (size_t i = 0; i < coef.size(); ++i) { cf[2 * i] = (float)coef[i].real(); cf[2 * i + 1] = (float)coef[i].imag(); }
+  } else {
+    double* cf = (double*)(prog.bytes.data() + hdr.off_coef);
+    for (size_t i = 0; i < coef.size(); ++i) { cf[2 * i] = coef[i].real(); cf[2 * i + 1] = coef[i].imag(); }
+  }
+  prog.structure_hash = h;
+  prog.npass = (int)pd.size();
+  prog.threads = threads;
+  prog.max_smem = smem;
+  return prog;
+}
+
+// ---------------------------------------------------------------------------------
+// Host interpretation of a program: gate semantics by physical bit, no thread mapping.
+// ---------------------------------------------------------------------------------
+template <typename R>
+static void emulate_t(const uint8_t* prog, std::complex<R>* psi, int n) {
+  using C = std::complex<R>;
+  const ProgramHeader* hdr = (const ProgramHeader*)prog;
+  const PassDesc* pd = (const PassDesc*)(prog + hdr->off_pass);
+  const PhaseDesc* phd = (const PhaseDesc*)(prog + hdr->off_phase);
+  const GateInstr* gi = (const GateInstr*)(prog + hdr->off_gate);
+  const C* cf = (const C*)(prog + hdr->off_coef);
+  const uint64_t dim = 1ull << n;
+  std::vector<C> tmp;
+  for (int p = 0; p < hdr->npass; ++p) {
+    const PassDesc& d = pd[p];
+    for (int h = 0; h < d.nphase; ++h) {
+      const PhaseDesc& ph = phd[d.phase0 + h];
+      auto phys = [&](uint8_t o) -> int { return o >= kFixed ? o - kFixed : d.sbit[ph.rbit[o]]; };
+      for (int g = 0; g < ph.ngate; ++g) {
+        const GateInstr& G = gi[ph.gate0 + g];
+        const C* c = cf + G.coef;
+        const int a = phys(G.a);
+        const uint64_t ma = 1ull << a;
+        switch (G.kind) {
+          case GK_1Q_DENSE: case GK_1Q_REAL: case GK_1Q_REIM:
+            for (uint64_t i = 0; i < dim; ++i) if (!(i & ma)) {
+              C x0 = psi[i], x1 = psi[i | ma];
+              psi[i] = c[0] * x0 + c[1] * x1; psi[i | ma] = c[2] * x0 + c[3] * x1;
+            }
+            break;
+          case GK_1Q_DIAG:
+            for (uint64_t i = 0; i < dim; ++i) psi[i] *= (i & ma) ? c[1] : c[0];
+            break;
+          case GK_1Q_X:
+            for (uint64_t i = 0; i < dim; ++i) if (!(i & ma)) std::swap(psi[i], psi[i | ma]);
+            break;
+          default: {
+            const int b = phys(G.b);
+            const uint64_t mb = 1ull << b;
+            if (G.kind == GK_2Q_DIAG) {
+              for (uint64_t i = 0; i < dim; ++i) psi[i] *= c[((i & ma) ? 1 : 0) + ((i & mb) ? 2 : 0)];
+            } else if (G.kind == GK_2Q_CX) {
+              for (uint64_t i = 0; i < dim; ++i) if ((i & ma) && !(i & mb)) std::swap(psi[i], psi[i | mb]);
+            } else if (G.kind == GK_2Q_CU) {
+              for (uint64_t i = 0; i < dim; ++i) if ((i & ma) && !(i & mb)) {
+                C x0 = psi[i], x1 = psi[i | mb];
+                psi[i] = c[0] * x0 + c[1] * x1; psi[i | mb] = c[2] * x0 + c[3] * x1;
+              }
+            } else if (G.kind == GK_2Q_SWAP) {
+              for (uint64_t i = 0; i < dim; ++i) if ((i & ma) && !(i & mb)) std::swap(psi[i], psi[(i ^ ma) | mb]);
+            } else if (G.kind == GK_2Q_DENSE) {
+              for (uint64_t i = 0; i < dim; ++i) if (!(i & ma) && !(i & mb)) {
+                const uint64_t idx[4] = {i, i | ma, i | mb, i | ma | mb};
+                C x[4] = {psi[idx[0]], psi[idx[1]], psi[idx[2]], psi[idx[3]]};
+                for (int rr = 0; rr < 4; ++rr)
+                  psi[idx[rr]] = c[4 * rr] * x[0] + c[4 * rr + 1] * x[1] + c[4 * rr + 2] * x[2] + c[4 * rr + 3] * x[3];
+              }
+            } else {
+              throw std::runtime_error("emulator: unknown gate kind");
+            }
+          }
+        }
+      }
+    }
+    if (d.store_perm) {
+      tmp.assign(psi, psi + dim);
+      // output local bit j takes input local bit store_src[j]
+      for (uint64_t i = 0; i < dim; ++i) {
+        uint64_t o = i;
+        for (int j = 0; j < d.m; ++j) o &= ~(1ull << d.sbit[j]);
+        for (int j = 0; j < d.m; ++j)
+          if (i & (1ull << d.sbit[d.store_src[j]])) o |= 1ull << d.sbit[j];
+        psi[o] = tmp[i];
+      }
+    }
+  }
+}
+
+void emulate_program(const uint8_t* prog, void* state, int n, int dtype) {
+  if (dtype == 0) emulate_t<float>(prog, (std::complex<float>*)state, n);
+  else emulate_t<double>(prog, (std::complex<double>*)state, n);
+}
+
+}  // namespace qsb

@@ -1,0 +1,88 @@
+// Host-side planning for the pass kernel: classification of gates, pass (sweep)
+// selection, register-phase selection, in-place permutation decomposition and the
+// encoding of a device program.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "qsim.h"
+
+namespace qsb {
+
+using cplx = std::complex<double>;
+
+// A gate queued for execution, at physical bits.
+struct QOp {
+  int arity = 1;          // 1 or 2
+  int q0 = 0, q1 = -1;    // physical bits; matrix index b_q0 + 2 b_q1
+  cplx U[16];             // row-major 2x2 (first 4) or 4x4
+};
+
+// A gate after classification (see GateKind).
+struct COp {
+  GateKind kind = GK_NONE;
+  int a = -1, b = -1;     // physical bits in role order
+  int ncoef = 0;
+  cplx coef[16];
+  uint64_t touch = 0;     // physical bits read or written
+  uint64_t need = 0;      // physical bits that must be staged (pass) / held in registers (phase)
+};
+
+COp classify(const QOp& op);
+
+struct PlanConfig {
+  int m = 13;             // local bits per pass
+  int r = 5;              // register bits per thread
+  int k = 3;              // lowest physical bits always staged (contiguous runs of 2^k amplitudes)
+  int hill_iters = 4;     // hill-climbing rounds when choosing the staged / register sets
+};
+
+struct PlannedPhase {
+  std::vector<int> rbits;  // local bits held in registers
+  std::vector<int> ops;    // indices into the op list, in execution order
+};
+
+struct PlannedPass {
+  std::vector<int> sbits;        // staged physical bits (ascending), size m
+  std::vector<int> ops;          // op indices in execution order
+  std::vector<PlannedPhase> phases;
+  std::vector<int> store_src;    // optional: output local bit j <- input local bit store_src[j]
+};
+
+// Split ops (in order) into passes and phases.
+std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const PlanConfig& cfg);
+
+// In-place bit permutation as a sequence of gate-free passes.  perm[b] = destination
+// physical bit of the data now at physical bit b.
+std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, const PlanConfig& cfg);
+
+// Encoded program (host copy) and its structure hash (coefficient values excluded).
+struct Program {
+  std::vector<uint8_t> bytes;
+  uint64_t structure_hash = 0;
+  int npass = 0;
+  int threads = 0;        // block size (max over passes of 2^(m - r))
+  size_t max_smem = 0;    // bytes of shared memory per block
+};
+
+Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops,
+                       int n, int dtype);
+
+// Reference interpretation of a program on host memory (used by CPU tests of the planner).
+void emulate_program(const uint8_t* prog, void* state, int n, int dtype);
+
+// Bank-spreading swizzle of a local amplitude index inside the shared-memory group.
+// complex64: XOR bits 1..3 with a fold of bits 4.. (bit 0 kept so aligned pairs stay together);
+// complex128: XOR bits 0..2 with a fold of bits 3..
+__host__ __device__ inline uint32_t swz64(uint32_t l) {
+  uint32_t f = (l >> 4) ^ (l >> 7) ^ (l >> 10) ^ (l >> 13);
+  return l ^ ((f & 7u) << 1);
+}
+__host__ __device__ inline uint32_t swz128(uint32_t l) {
+  uint32_t f = (l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12);
+  return l ^ (f & 7u);
+}
+
+}  // namespace qsb

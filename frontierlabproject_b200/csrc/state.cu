@@ -1,0 +1,695 @@
+// State handle and C ABI of libqsim_b200 (see include/qsim_b200.h).
+//
+// Execution model
+//  * permute() only relabels: pos2bit[p] is the physical bit that holds layout position p.
+//  * Tile ops in cooperative/graphed mode are queued at physical bits and run when the
+//    state is next observed (copy-out, synchronize, device pointer, reductions) or when a
+//    sequential op arrives.  The queue is planned into passes (pass kernel); cooperative
+//    mode runs all passes in one persistent launch with bounded grid barriers, graphed
+//    mode replays a cached CUDA graph of one launch per pass.
+//  * Observation first moves the data to the current layout with in-place permutation
+//    passes (bit-exact), so pos2bit becomes the identity.
+#include <algorithm>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/qsim_b200.h"
+#include "kernels.h"
+#include "plan.h"
+#include "qsim.h"
+
+using namespace qsb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+struct CudaError {
+  cudaError_t e;
+};
+
+#define CK(call)                                    \
+  do {                                              \
+    cudaError_t _e = (call);                        \
+    if (_e != cudaSuccess) throw CudaError{_e};     \
+  } while (0)
+
+struct InvalidArg {
+  std::string msg;
+};
+
+constexpr uint64_t kBarrierLimitNs = 20ull * 1000ull * 1000ull * 1000ull;  // 20 s
+
+int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
+
+}  // namespace
+
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  uint64_t key = 0;
+};
+
+struct qs_state {
+  int n = 0;
+  int dtype = 0;
+  size_t esz = 8;
+  uint64_t dim = 0;
+  void* psi = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  std::vector<int> pos2bit;
+  std::vector<QOp> queue;
+  int queue_mode = QS_MODE_COOPERATIVE;
+  PlanConfig cfg;
+  int grid_mult = 0;
+  // device scratch: program buffer, control words (barrier x2, error), accumulators
+  uint8_t* d_prog = nullptr;
+  size_t prog_cap = 0;
+  uint8_t* h_prog = nullptr;  // pinned staging of the program
+  size_t hprog_cap = 0;
+  cudaEvent_t prog_copied = nullptr;
+  unsigned* d_ctl = nullptr;
+  double* d_acc = nullptr;
+  double* h_acc = nullptr;    // pinned
+  GraphEntry graph;
+  qs_stats st{};
+
+  ~qs_state() {
+    if (graph.exec) cudaGraphExecDestroy(graph.exec);
+    if (psi) cudaFree(psi);
+    if (d_prog) cudaFree(d_prog);
+    if (h_prog) cudaFreeHost(h_prog);
+    if (h_acc) cudaFreeHost(h_acc);
+    if (d_ctl) cudaFree(d_ctl);
+    if (d_acc) cudaFree(d_acc);
+    if (prog_copied) cudaEventDestroy(prog_copied);
+    if (stream && own_stream) cudaStreamDestroy(stream);
+  }
+
+  bool identity_layout() const {
+    for (int p = 0; p < n; ++p) if (pos2bit[p] != p) return false;
+    return true;
+  }
+
+  void ensure_prog(size_t bytes) {
+    if (bytes > prog_cap) {
+      CK(cudaStreamSynchronize(stream));
+      if (d_prog) CK(cudaFree(d_prog));
+      prog_cap = std::max<size_t>(bytes * 2, 1 << 16);
+      CK(cudaMalloc(&d_prog, prog_cap));
+      if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
+    }
+    if (bytes > hprog_cap) {
+      CK(cudaEventSynchronize(prog_copied));
+      if (h_prog) CK(cudaFreeHost(h_prog));
+      hprog_cap = std::max<size_t>(bytes * 2, 1 << 16);
+      CK(cudaMallocHost(&h_prog, hprog_cap));
+    }
+  }
+
+  // copy the encoded program to the device (ordered on the stream)
+  void upload(const Program& prog) {
+    ensure_prog(prog.bytes.size());
+    CK(cudaEventSynchronize(prog_copied));  // previous upload finished reading h_prog
+    std::memcpy(h_prog, prog.bytes.data(), prog.bytes.size());
+    CK(cudaMemcpyAsync(d_prog, h_prog, prog.bytes.size(), cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(prog_copied, stream));
+  }
+
+  int grid_for_program(const Program& prog) {
+    int per_sm = 1;
+    CK(pass_kernel_occupancy(dtype, prog.threads, prog.max_smem, &per_sm));
+    if (per_sm < 1) throw InvalidArg{"pass kernel does not fit on an SM"};
+    if (grid_mult > 0) per_sm = std::min(per_sm, grid_mult);
+    return per_sm * device_sm_count();
+  }
+
+  void run_program(const Program& prog, int mode) {
+    if (prog.npass == 0) return;
+    upload(prog);
+    int grid = grid_for_program(prog);
+    if (mode == QS_MODE_COOPERATIVE) {
+      CK(cudaMemsetAsync(d_ctl, 0, 2 * sizeof(unsigned), stream));
+      CK(launch_pass_kernel(dtype, d_prog, psi, 0, prog.npass, prog.threads, prog.max_smem, grid, true, d_ctl,
+                            d_ctl + 2, kBarrierLimitNs, stream));
+      st.launches += 1;
+    } else {
+      const uint64_t key = prog.structure_hash ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
+                           ((uint64_t)(uintptr_t)d_prog << 1) ^ (uint64_t)grid;
+      if (!graph.exec || graph.key != key) {
+        if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int p = 0; p < prog.npass && e == cudaSuccess; ++p)
+          e = launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false, d_ctl,
+                                 d_ctl + 2, kBarrierLimitNs, stream);
+        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
+        if (e2 != cudaSuccess) throw CudaError{e2};
+        cudaError_t e3 = cudaGraphInstantiate(&graph.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) throw CudaError{e3};
+        graph.key = key;
+        st.graph_builds += 1;
+      } else {
+        st.graph_replays += 1;
+      }
+      CK(cudaGraphLaunch(graph.exec, stream));
+      st.launches += 1;
+    }
+    st.sweeps += prog.npass;
+  }
+
+  bool use_pass_kernel() const { return n >= reg_bits(dtype) + 1; }
+
+  PlanConfig eff_cfg() const {
+    PlanConfig c = cfg;
+    c.r = reg_bits(dtype);
+    c.m = std::max(c.r, std::min(c.m, n));
+    return c;
+  }
+
+  void run_ops_sequential(const std::vector<QOp>& ops) {
+    for (const QOp& o : ops) {
+      if (o.arity == 1) CK(launch_gate1(dtype, psi, n, o.q0, o.U, stream));
+      else CK(launch_gate2(dtype, psi, n, o.q0, o.q1, o.U, stream));
+      st.launches += 1;
+      st.gate_sweeps += 1;
+    }
+  }
+
+  void flush() {
+    if (queue.empty()) return;
+    std::vector<QOp> ops;
+    ops.swap(queue);
+    st.flushes += 1;
+    if (!use_pass_kernel() || queue_mode == QS_MODE_SEQUENTIAL) {
+      run_ops_sequential(ops);
+      return;
+    }
+    std::vector<COp> cops;
+    cops.reserve(ops.size());
+    for (const QOp& o : ops) cops.push_back(classify(o));
+    PlanConfig c = eff_cfg();
+    auto passes = plan_passes(cops, n, c);
+    Program prog = encode_program(passes, cops, n, dtype);
+    run_program(prog, queue_mode);
+  }
+
+  // move data so that physical bit p holds layout position p
+  void materialize() {
+    flush();
+    if (identity_layout()) return;
+    std::vector<int> perm(n);
+    for (int p = 0; p < n; ++p) perm[pos2bit[p]] = p;
+    if (!use_pass_kernel()) {
+      // tiny states: out-of-place scatter through a temporary buffer
+      void* tmp = nullptr;
+      CK(cudaMallocAsync(&tmp, dim * esz, stream));
+      CK(launch_permute_scatter(dtype, psi, tmp, n, perm.data(), stream));
+      CK(cudaMemcpyAsync(psi, tmp, dim * esz, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaFreeAsync(tmp, stream));
+      st.launches += 1;
+    } else {
+      PlanConfig c = eff_cfg();
+      auto passes = plan_permutation(perm, n, c);
+      std::vector<COp> none;
+      Program prog = encode_program(passes, none, n, dtype);
+      run_program(prog, QS_MODE_COOPERATIVE);
+      st.perm_sweeps += prog.npass;
+    }
+    for (int p = 0; p < n; ++p) pos2bit[p] = p;
+  }
+
+  void check_device_error() {
+    unsigned w[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(w, d_ctl, sizeof(w), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (w[2] != 0) {
+      CK(cudaMemsetAsync(d_ctl, 0, 3 * sizeof(unsigned), stream));
+      throw InvalidArg{"device error: a grid barrier wait expired (error word " + std::to_string(w[2]) + ")"};
+    }
+  }
+
+  void sync() {
+    flush();
+    CK(cudaStreamSynchronize(stream));
+    check_device_error();
+  }
+};
+
+// ------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------
+namespace {
+
+template <typename F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const InvalidArg& e) {
+    return fail(QS_ERR_INVALID, e.msg);
+  } catch (const CudaError& e) {
+    return fail(QS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e.e));
+  } catch (const std::exception& e) {
+    return fail(QS_ERR_INVALID, e.what());
+  }
+}
+
+void read_matrix(const qs_state* s, int dtype, const void* U, int u_on_device, int count, cplx* out) {
+  const size_t esz = dtype == 0 ? 8 : 16;
+  std::vector<uint8_t> buf(count * esz);
+  const void* src = U;
+  if (u_on_device) {
+    CK(cudaMemcpy(buf.data(), U, count * esz, cudaMemcpyDeviceToHost));
+    src = buf.data();
+  }
+  if (dtype == 0) {
+    const float* f = (const float*)src;
+    for (int i = 0; i < count; ++i) out[i] = cplx(f[2 * i], f[2 * i + 1]);
+  } else {
+    const double* f = (const double*)src;
+    for (int i = 0; i < count; ++i) out[i] = cplx(f[2 * i], f[2 * i + 1]);
+  }
+  (void)s;
+}
+
+// validate a tile op list like parse_tile_ops (bindings.cpp:182-220) and convert it
+std::vector<QOp> convert_ops(const qs_state* s, const qs_op* ops, int nops, int n, int dtype, bool map_layout) {
+  std::vector<QOp> out;
+  out.reserve(nops);
+  for (int i = 0; i < nops; ++i) {
+    const qs_op& o = ops[i];
+    QOp q;
+    if (o.kind == QS_OP_1Q) {
+      if (o.q0 < 0 || o.q0 >= n) throw InvalidArg{"apply_tile_dev: invalid q0"};
+      if (!o.U) throw InvalidArg{"apply_tile_dev: null gate matrix"};
+      q.arity = 1;
+      q.q0 = map_layout ? s->pos2bit[o.q0] : o.q0;
+      read_matrix(s, dtype, o.U, o.u_on_device, 4, q.U);
+    } else if (o.kind == QS_OP_2Q) {
+      if (o.q0 < 0 || o.q0 >= n || o.q1 < 0 || o.q1 >= n) throw InvalidArg{"apply_tile_dev: invalid q0/q1"};
+      if (o.q0 == o.q1) throw InvalidArg{"apply_tile_dev: q0 == q1"};
+      if (!o.U) throw InvalidArg{"apply_tile_dev: null gate matrix"};
+      q.arity = 2;
+      q.q0 = map_layout ? s->pos2bit[o.q0] : o.q0;
+      q.q1 = map_layout ? s->pos2bit[o.q1] : o.q1;
+      read_matrix(s, dtype, o.U, o.u_on_device, 16, q.U);
+    } else {
+      throw InvalidArg{"apply_tile_dev: unknown op kind: " + std::to_string(o.kind)};
+    }
+    out.push_back(q);
+  }
+  return out;
+}
+
+void enqueue(qs_state* s, std::vector<QOp>&& ops, int mode) {
+  if (ops.empty()) return;
+  s->st.gates += ops.size();
+  if (mode == QS_MODE_SEQUENTIAL) {
+    s->flush();
+    s->run_ops_sequential(ops);
+    return;
+  }
+  if (!s->queue.empty() && s->queue_mode != mode) s->flush();
+  s->queue_mode = mode;
+  for (auto& o : ops) s->queue.push_back(o);
+  if (s->queue.size() > 200000) s->flush();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------
+extern "C" {
+
+const char* qs_last_error(void) { return g_err.c_str(); }
+int qs_version(void) { return 100; }
+
+int qs_device_count(int* out) {
+  return guard([&] {
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) c = 0;
+    *out = c;
+  });
+}
+
+int qs_create(int num_qubits, int dtype, qs_state** out) {
+  return guard([&] {
+    if (!out) throw InvalidArg{"null output handle"};
+    *out = nullptr;
+    if (dtype != QS_C64 && dtype != QS_C128) throw InvalidArg{"dtype must be QS_C64 or QS_C128"};
+    if (num_qubits < 1 || num_qubits > 36) throw InvalidArg{"num_qubits must be in [1, 36]"};
+    std::unique_ptr<qs_state> s(new qs_state());
+    s->n = num_qubits;
+    s->dtype = dtype;
+    s->esz = dtype == 0 ? 8 : 16;
+    s->dim = 1ull << num_qubits;
+    s->cfg.m = dtype == 0 ? 13 : 12;
+    s->cfg.k = 3;
+    s->pos2bit.resize(num_qubits);
+    for (int p = 0; p < num_qubits; ++p) s->pos2bit[p] = p;
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s->prog_copied, cudaEventDisableTiming));
+    CK(cudaMalloc(&s->psi, s->dim * s->esz));
+    CK(cudaMalloc(&s->d_ctl, 4 * sizeof(unsigned)));
+    CK(cudaMalloc(&s->d_acc, 8 * sizeof(double)));
+    CK(cudaMallocHost(&s->h_acc, 8 * sizeof(double)));
+    CK(cudaMemsetAsync(s->d_ctl, 0, 4 * sizeof(unsigned), s->stream));
+    CK(launch_set_basis(dtype, s->psi, num_qubits, 0, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    *out = s.release();
+  });
+}
+
+int qs_destroy(qs_state* s) {
+  return guard([&] {
+    if (!s) return;
+    cudaStreamSynchronize(s->stream);
+    delete s;
+  });
+}
+
+int qs_num_qubits(const qs_state* s, int* out) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; *out = s->n; });
+}
+int qs_dim(const qs_state* s, unsigned long long* out) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; *out = s->dim; });
+}
+int qs_dtype(const qs_state* s, int* out) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; *out = s->dtype; });
+}
+
+int qs_reset(qs_state* s) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    s->queue.clear();
+    for (int p = 0; p < s->n; ++p) s->pos2bit[p] = p;
+    CK(launch_set_basis(s->dtype, s->psi, s->n, 0, s->stream));
+    s->st.launches += 1;
+  });
+}
+
+int qs_synchronize(qs_state* s) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    s->sync();
+  });
+}
+
+int qs_copy_to_host(qs_state* s, void* dst, unsigned long long nbytes) {
+  return guard([&] {
+    if (!s || !dst) throw InvalidArg{"null argument"};
+    if (nbytes != s->dim * s->esz) throw InvalidArg{"Output array must have size 2^num_qubits"};
+    s->materialize();
+    CK(cudaMemcpyAsync(dst, s->psi, nbytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->check_device_error();
+  });
+}
+
+int qs_copy_from_host(qs_state* s, const void* src, unsigned long long nbytes) {
+  return guard([&] {
+    if (!s || !src) throw InvalidArg{"null argument"};
+    if (nbytes != s->dim * s->esz) throw InvalidArg{"Input array must have size 2^num_qubits"};
+    s->flush();
+    for (int p = 0; p < s->n; ++p) s->pos2bit[p] = p;
+    CK(cudaMemcpyAsync(s->psi, src, nbytes, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+  });
+}
+
+int qs_permute(qs_state* s, const int* layout_old, const int* layout_new, int n) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    if (n != s->n || !layout_old || !layout_new)
+      throw InvalidArg{"layout_old/layout_new must have length num_qubits"};
+    std::vector<int> new_pos(n, -1), old_seen(n, 0), map(n, -1);
+    for (int p = 0; p < n; ++p) {
+      int gq = layout_new[p];
+      if (gq < 0 || gq >= n) throw InvalidArg{"layout_new contains invalid qubit id"};
+      if (new_pos[gq] != -1) throw InvalidArg{"layout_new is not a permutation"};
+      new_pos[gq] = p;
+    }
+    for (int p = 0; p < n; ++p) {
+      int gq = layout_old[p];
+      if (gq < 0 || gq >= n) throw InvalidArg{"layout_old contains invalid qubit id"};
+      if (old_seen[gq]++) throw InvalidArg{"layout_old is not a permutation"};
+      map[p] = new_pos[gq];
+    }
+    // scatter semantics: data at position p moves to position map[p]
+    std::vector<int> nb(n);
+    for (int p = 0; p < n; ++p) nb[map[p]] = s->pos2bit[p];
+    s->pos2bit.swap(nb);
+    s->st.permutes += 1;
+  });
+}
+
+int qs_apply_tile(qs_state* s, const qs_op* ops, int nops, int mode) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    if (mode < 0 || mode > 2) throw InvalidArg{"unknown tile mode"};
+    if (nops < 0 || (nops > 0 && !ops)) throw InvalidArg{"invalid op list"};
+    enqueue(s, convert_ops(s, ops, nops, s->n, s->dtype, true), mode);
+  });
+}
+
+int qs_apply_1q(qs_state* s, int target_qubit, const void* U, int u_on_device) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    if (target_qubit < 0 || target_qubit >= s->n) throw InvalidArg{"Invalid target qubit"};
+    if (!U) throw InvalidArg{"U must be a 2x2 matrix"};
+    qs_op o{QS_OP_1Q, target_qubit, -1, u_on_device, U};
+    enqueue(s, convert_ops(s, &o, 1, s->n, s->dtype, true), QS_MODE_SEQUENTIAL);
+  });
+}
+
+int qs_apply_2q(qs_state* s, int q0, int q1, const void* U, int u_on_device) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    if (q0 < 0 || q0 >= s->n || q1 < 0 || q1 >= s->n) throw InvalidArg{"Invalid qubit indices"};
+    if (q0 == q1) throw InvalidArg{"q0 and q1 must be different"};
+    if (!U) throw InvalidArg{"U must be a 4x4 matrix"};
+    qs_op o{QS_OP_2Q, q0, q1, u_on_device, U};
+    enqueue(s, convert_ops(s, &o, 1, s->n, s->dtype, true), QS_MODE_SEQUENTIAL);
+  });
+}
+
+int qs_apply_diagonal_1q(qs_state* s, int target_qubit, const double* phase0, const double* phase1) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    if (target_qubit < 0 || target_qubit >= s->n) throw InvalidArg{"Invalid target qubit"};
+    s->flush();
+    CK(launch_diag1(s->dtype, s->psi, s->n, s->pos2bit[target_qubit], cplx(phase0[0], phase0[1]),
+                    cplx(phase1[0], phase1[1]), s->stream));
+    s->st.gates += 1;
+    s->st.launches += 1;
+    s->st.gate_sweeps += 1;
+  });
+}
+
+int qs_flush(qs_state* s) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; s->flush(); });
+}
+
+int qs_device_ptr(qs_state* s, void** out) {
+  return guard([&] {
+    if (!s || !out) throw InvalidArg{"null argument"};
+    s->materialize();
+    s->sync();
+    *out = s->psi;
+  });
+}
+
+int qs_set_stream(qs_state* s, void* stream) {
+  return guard([&] {
+    if (!s) throw InvalidArg{"null state"};
+    s->flush();
+    CK(cudaStreamSynchronize(s->stream));
+    if (s->own_stream) CK(cudaStreamDestroy(s->stream));
+    if (stream) {
+      s->stream = (cudaStream_t)stream;
+      s->own_stream = false;
+    } else {
+      CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+      s->own_stream = true;
+    }
+    if (s->graph.exec) { cudaGraphExecDestroy(s->graph.exec); s->graph.exec = nullptr; }
+  });
+}
+
+int qs_get_stream(qs_state* s, void** out) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; *out = (void*)s->stream; });
+}
+
+int qs_set_config(qs_state* s, const qs_config* c) {
+  return guard([&] {
+    if (!s || !c) throw InvalidArg{"null argument"};
+    const int mmax = s->dtype == 0 ? 13 : 12;
+    if (c->m < reg_bits(s->dtype) + 1 || c->m > mmax) throw InvalidArg{"config: m out of range"};
+    if (c->k < 1 || c->k > c->m) throw InvalidArg{"config: k out of range"};
+    if (c->hill_iters < 0) throw InvalidArg{"config: hill_iters must be >= 0"};
+    s->flush();
+    s->cfg.m = c->m;
+    s->cfg.k = c->k;
+    s->cfg.hill_iters = c->hill_iters;
+    s->grid_mult = c->grid_mult;
+  });
+}
+
+int qs_get_config(qs_state* s, qs_config* c) {
+  return guard([&] {
+    if (!s || !c) throw InvalidArg{"null argument"};
+    c->m = s->cfg.m; c->k = s->cfg.k; c->hill_iters = s->cfg.hill_iters; c->grid_mult = s->grid_mult;
+  });
+}
+
+int qs_get_stats(qs_state* s, qs_stats* out) {
+  return guard([&] { if (!s || !out) throw InvalidArg{"null argument"}; *out = s->st; });
+}
+int qs_reset_stats(qs_state* s) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; s->st = qs_stats{}; });
+}
+int qs_get_pos2bit(qs_state* s, int* out, int n) {
+  return guard([&] {
+    if (!s || !out || n != s->n) throw InvalidArg{"bad arguments"};
+    for (int p = 0; p < n; ++p) out[p] = s->pos2bit[p];
+  });
+}
+
+int qs_norm_squared(qs_state* s, double* out) {
+  return guard([&] {
+    if (!s || !out) throw InvalidArg{"null argument"};
+    s->flush();
+    CK(cudaMemsetAsync(s->d_acc, 0, sizeof(double), s->stream));
+    CK(launch_norm2(s->dtype, s->psi, s->n, s->d_acc, s->stream));
+    CK(cudaMemcpyAsync(s->h_acc, s->d_acc, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->check_device_error();
+    *out = s->h_acc[0];
+  });
+}
+
+int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im) {
+  return guard([&] {
+    if (!a || !b || !re || !im) throw InvalidArg{"null argument"};
+    if (a->n != b->n || a->dtype != b->dtype) throw InvalidArg{"states differ in size or dtype"};
+    a->materialize();
+    b->materialize();
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaMemsetAsync(a->d_acc, 0, 2 * sizeof(double), a->stream));
+    CK(launch_inner(a->dtype, a->psi, b->psi, a->n, a->d_acc, a->stream));
+    CK(cudaMemcpyAsync(a->h_acc, a->d_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
+    CK(cudaStreamSynchronize(a->stream));
+    a->check_device_error();
+    *re = a->h_acc[0];
+    *im = a->h_acc[1];
+  });
+}
+
+int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream) {
+  return guard([&] {
+    if (!psi || !U) throw InvalidArg{"null argument"};
+    if (dtype != 0 && dtype != 1) throw InvalidArg{"dtype must be QS_C64 or QS_C128"};
+    if (num_qubits < 1 || num_qubits > 36) throw InvalidArg{"num_qubits must be in [1, 36]"};
+    if (target_qubit < 0 || target_qubit >= num_qubits) throw InvalidArg{"Invalid target qubit"};
+    cplx m[4];
+    read_matrix(nullptr, dtype, U, 0, 4, m);
+    CK(launch_gate1(dtype, psi, num_qubits, target_qubit, m, (cudaStream_t)stream));
+  });
+}
+
+int qs_apply_2q_gate(void* psi, int dtype, const void* U, int q0, int q1, int num_qubits, void* stream) {
+  return guard([&] {
+    if (!psi || !U) throw InvalidArg{"null argument"};
+    if (dtype != 0 && dtype != 1) throw InvalidArg{"dtype must be QS_C64 or QS_C128"};
+    if (num_qubits < 2 || num_qubits > 36) throw InvalidArg{"num_qubits must be in [2, 36]"};
+    if (q0 < 0 || q0 >= num_qubits || q1 < 0 || q1 >= num_qubits) throw InvalidArg{"Invalid qubit indices"};
+    if (q0 == q1) throw InvalidArg{"q0 and q1 must be different"};
+    cplx m[16];
+    read_matrix(nullptr, dtype, U, 0, 16, m);
+    CK(launch_gate2(dtype, psi, num_qubits, q0, q1, m, (cudaStream_t)stream));
+  });
+}
+
+int qs_permute_scatter(const void* in, void* out, int dtype, int num_qubits, const int* map, void* stream) {
+  return guard([&] {
+    if (!in || !out || !map) throw InvalidArg{"null argument"};
+    if (num_qubits < 1 || num_qubits > 36) throw InvalidArg{"num_qubits must be in [1, 36]"};
+    std::vector<int> seen(num_qubits, 0);
+    for (int p = 0; p < num_qubits; ++p) {
+      if (map[p] < 0 || map[p] >= num_qubits || seen[map[p]]++) throw InvalidArg{"map is not a permutation"};
+    }
+    CK(launch_permute_scatter(dtype, in, out, num_qubits, map, (cudaStream_t)stream));
+  });
+}
+
+// ---- host-only planner inspection -----------------------------------------------------
+static PlanConfig cfg_from(int dtype, int n, const qs_config* c) {
+  PlanConfig p;
+  p.r = reg_bits(dtype);
+  p.m = c ? c->m : (dtype == 0 ? 13 : 12);
+  p.k = c ? c->k : 3;
+  p.hill_iters = c ? c->hill_iters : 4;
+  p.m = std::max(p.r, std::min(p.m, n));
+  return p;
+}
+
+int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps,
+                 int* phases) {
+  return guard([&] {
+    if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
+    auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
+    std::vector<COp> c;
+    for (auto& o : q) c.push_back(classify(o));
+    auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
+    int ph = 0;
+    for (auto& p : passes) ph += (int)p.phases.size();
+    if (sweeps) *sweeps = (int)passes.size();
+    if (phases) *phases = ph;
+  });
+}
+
+int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg, void* psi) {
+  return guard([&] {
+    if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 24) throw InvalidArg{"num_qubits out of range"};
+    auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
+    std::vector<COp> c;
+    for (auto& o : q) c.push_back(classify(o));
+    auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
+    Program prog = encode_program(passes, c, num_qubits, dtype);
+    emulate_program(prog.bytes.data(), psi, num_qubits, dtype);
+  });
+}
+
+int qs_perm_emulate(int num_qubits, int dtype, const int* perm, const qs_config* cfg, void* psi, int* sweeps) {
+  return guard([&] {
+    if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 24) throw InvalidArg{"num_qubits out of range"};
+    std::vector<int> p(perm, perm + num_qubits), seen(num_qubits, 0);
+    for (int b = 0; b < num_qubits; ++b)
+      if (p[b] < 0 || p[b] >= num_qubits || seen[p[b]]++) throw InvalidArg{"perm is not a permutation"};
+    auto passes = plan_permutation(p, num_qubits, cfg_from(dtype, num_qubits, cfg));
+    std::vector<COp> none;
+    Program prog = encode_program(passes, none, num_qubits, dtype);
+    emulate_program(prog.bytes.data(), psi, num_qubits, dtype);
+    if (sweeps) *sweeps = prog.npass;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+/*
+ * libqsim_b200 -- C ABI of the B200 statevector tile executor.
+ *
+ * Drop-in boundary for the native module of qgpusim's custom backend
+ * (pybind11 module ``qgpusim_cuda``, qgpusim/backends/custom/qgpusim_cuda/src/bindings.cpp:1004-1092).
+ * Every function returns 0 on success or a negative status; the message of the last
+ * failure on the calling thread is returned by qs_last_error().  Message texts follow the
+ * reference's std::runtime_error messages where the reference has one.
+ *
+ * Complex numbers are interleaved (re, im) in the state's precision unless stated:
+ * QS_C64 = complex64 (StatevectorF32), QS_C128 = complex128 (Statevector).
+ * Gate matrices are row-major; for 2-qubit gates the index is b_q0 + 2*b_q1
+ * (kernels.cu:54-55,108-114).  Qubit arguments of tile ops are bit positions in the
+ * state's current layout (after permute()).
+ */
+#ifndef QSIM_B200_H
+#define QSIM_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define QS_API __attribute__((visibility("default")))
+#else
+#define QS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QS_C64 0
+#define QS_C128 1
+
+#define QS_MODE_COOPERATIVE 0 /* apply_tile_cooperative */
+#define QS_MODE_GRAPHED 1     /* apply_tile_graphed     */
+#define QS_MODE_SEQUENTIAL 2  /* apply_tile_dev         */
+
+#define QS_OP_1Q 1
+#define QS_OP_2Q 2
+
+#define QS_ERR_INVALID -1 /* bad argument */
+#define QS_ERR_CUDA -2    /* CUDA runtime error */
+#define QS_ERR_DEVICE -3  /* a kernel reported an error word (bounded wait expired) */
+
+typedef struct qs_state qs_state;
+
+/* One tile op: ('1q', q0, U) or ('2q', q0, q1, U) of bindings.cpp:182-220.
+ * U points to 4 or 16 complex entries in the state's precision; u_on_device = 1 when U
+ * is a device pointer.  The executor copies U before returning (no borrowed pointer). */
+typedef struct {
+  int kind; /* QS_OP_1Q or QS_OP_2Q */
+  int q0;
+  int q1;
+  int u_on_device;
+  const void* U;
+} qs_op;
+
+typedef struct {
+  int m;          /* local (staged) bits per sweep; c64 <= 13, c128 <= 12 */
+  int k;          /* lowest physical bits always staged (>= 1) */
+  int hill_iters; /* planner search effort */
+  int grid_mult;  /* resident blocks per SM used by the pass kernel (0 = occupancy) */
+} qs_config;
+
+typedef struct {
+  unsigned long long gates;          /* ops accepted */
+  unsigned long long sweeps;         /* full-state passes run by the pass kernel */
+  unsigned long long perm_sweeps;    /* of which: in-place permutation passes */
+  unsigned long long gate_sweeps;    /* per-gate kernel sweeps (sequential mode / per-gate API) */
+  unsigned long long launches;       /* kernel launches (graph launches count once) */
+  unsigned long long graph_replays;  /* cached graph launches */
+  unsigned long long graph_builds;   /* graph captures */
+  unsigned long long flushes;        /* planned executions */
+  unsigned long long permutes;       /* permute() calls */
+} qs_stats;
+
+/* Library */
+QS_API const char* qs_last_error(void);
+QS_API int qs_version(void);
+QS_API int qs_device_count(int* out);
+
+/* Statevector(num_qubits) / StatevectorF32(num_qubits): bindings.cpp:92-110, 645-658 */
+QS_API int qs_create(int num_qubits, int dtype, qs_state** out);
+/* ~Statevector: bindings.cpp:112-122 */
+QS_API int qs_destroy(qs_state* s);
+/* num_qubits / dim properties: bindings.cpp:1023-1024 */
+QS_API int qs_num_qubits(const qs_state* s, int* out);
+QS_API int qs_dim(const qs_state* s, unsigned long long* out);
+QS_API int qs_dtype(const qs_state* s, int* out);
+
+/* reset(): bindings.cpp:577-582 */
+QS_API int qs_reset(qs_state* s);
+/* synchronize(): bindings.cpp:585-587 (executes queued ops, waits, checks error words) */
+QS_API int qs_synchronize(qs_state* s);
+/* to_numpy(): bindings.cpp:547-560 -- state in the current layout, nbytes = dim * elem */
+QS_API int qs_copy_to_host(qs_state* s, void* dst, unsigned long long nbytes);
+/* from_numpy(psi): bindings.cpp:563-574 (also offered for complex64) */
+QS_API int qs_copy_from_host(qs_state* s, const void* src, unsigned long long nbytes);
+
+/* permute(layout_old, layout_new): bindings.cpp:434-483, scatter semantics of
+ * kernels.cu:165-185.  Recorded as a relabelling; data moves (in place, bit-exact) when
+ * the state is next observed. */
+QS_API int qs_permute(qs_state* s, const int* layout_old, const int* layout_new, int n);
+
+/* apply_tile_cooperative / apply_tile_graphed / apply_tile_dev: bindings.cpp:223-373 */
+QS_API int qs_apply_tile(qs_state* s, const qs_op* ops, int nops, int mode);
+/* apply_1q / apply_2q / apply_1q_dev / apply_2q_dev: bindings.cpp:499-544, 589-608 */
+QS_API int qs_apply_1q(qs_state* s, int target_qubit, const void* U, int u_on_device);
+QS_API int qs_apply_2q(qs_state* s, int q0, int q1, const void* U, int u_on_device);
+/* apply_diagonal_1q(target, phase0, phase1): bindings.cpp:611-619; phases complex128 */
+QS_API int qs_apply_diagonal_1q(qs_state* s, int target_qubit, const double* phase0, const double* phase1);
+
+/* Run queued ops now (asynchronously on the state's stream). */
+QS_API int qs_flush(qs_state* s);
+/* Device address of the amplitudes in the current layout (executes queued ops and
+ * pending data movement, then synchronises).  Valid until the next call on s. */
+QS_API int qs_device_ptr(qs_state* s, void** out);
+/* Stream used by s (cudaStream_t); NULL selects the state's own non-blocking stream. */
+QS_API int qs_set_stream(qs_state* s, void* stream);
+QS_API int qs_get_stream(qs_state* s, void** out);
+QS_API int qs_set_config(qs_state* s, const qs_config* cfg);
+QS_API int qs_get_config(qs_state* s, qs_config* cfg);
+QS_API int qs_get_stats(qs_state* s, qs_stats* out);
+QS_API int qs_reset_stats(qs_state* s);
+/* Current layout relabelling: out[p] = physical bit holding layout position p. */
+QS_API int qs_get_pos2bit(qs_state* s, int* out, int n);
+
+/* Reductions in FP64: sum |psi|^2 and <a|b> (states of equal size and dtype). */
+QS_API int qs_norm_squared(qs_state* s, double* out);
+QS_API int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im);
+
+/* Module-level apply_1q_gate / apply_2q_gate (bindings.cpp:931-1001): gate on a raw
+ * device array psi of 2^num_qubits amplitudes; U is a host matrix; stream may be NULL. */
+QS_API int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream);
+QS_API int qs_apply_2q_gate(void* psi, int dtype, const void* U, int q0, int q1, int num_qubits, void* stream);
+/* Reference permute kernel semantics on raw device arrays (out-of-place scatter,
+ * kernels.cu:165-185): out[sum_p bit_p(i) << map_old_to_new[p]] = in[i]. */
+QS_API int qs_permute_scatter(const void* in, void* out, int dtype, int num_qubits, const int* map_old_to_new,
+                       void* stream);
+
+/* Planner inspection (host only, no GPU needed): plan the ops of a tile list for an
+ * n-qubit state and report sweeps / phases.  ops use physical bits. */
+QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg,
+                 int* sweeps, int* phases);
+/* Host emulation of the planned program (tests of the planner, no GPU needed):
+ * applies ops to the host state psi (2^n entries, dtype precision). */
+QS_API int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg, void* psi);
+/* Host emulation of the in-place permutation program: perm[b] = destination bit. */
+QS_API int qs_perm_emulate(int num_qubits, int dtype, const int* perm, const qs_config* cfg, void* psi,
+                    int* sweeps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSIM_B200_H */

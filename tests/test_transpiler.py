@@ -1,0 +1,61 @@
+"""The LQR tiler reproduces the reference's tile schedules exactly."""
+import numpy as np
+import pytest
+
+from frontierlabproject_b200.transpiler import LazyQubitReordering, make_custom_pm, tile_circuit
+from frontierlabproject_b200.transpiler.passes import _build_tile_layout
+from tests.cases import BUILDERS, nl_of
+
+
+def _record(qc, plan):
+    pos = {(id(ins.operation), tuple(ins.qubits)): k for k, ins in enumerate(qc.data)}
+    return [{"tile_idx": t.tile_idx, "logical_qubits": list(t.logical_qubits), "layout": list(t.layout),
+             "gates": [pos[(id(g.op), tuple(g.qargs))] for g in t.gates]} for t in plan]
+
+
+@pytest.mark.parametrize("name", sorted(BUILDERS))
+def test_schedule_matches_reference(name, schedules):
+    qc = BUILDERS[name]()
+    nL = nl_of(name)
+    _, plan = tile_circuit(qc, nL)
+    assert _record(qc, plan) == schedules[name]["tiles"]
+
+
+def test_published_tile_counts(schedules):
+    # results/result.csv:6-8 (n=20) and :13-15 (n=25): 5 tiles / 4 reorders, 9 / 8
+    for name, tiles in [("u_layers_n20_d16_s42_nL16_save", 5), ("u_layers_n25_d16_s42_nL16_save", 9)]:
+        _, plan = tile_circuit(BUILDERS[name](), 16)
+        assert len(plan) == tiles
+        assert plan[-1].layout == list(range(plan[-1].layout.__len__()))  # forced all-qubit tile
+
+
+def test_layout_and_local_map():
+    assert _build_tile_layout([1, 4], 6) == [1, 4, 0, 2, 3, 5]
+    _, plan = tile_circuit(BUILDERS["random_layered_n12_d8_s2_nL8"](), 8)
+    for t in plan:
+        assert t.logical_qubits == sorted(t.logical_qubits)
+        assert t.layout[:len(t.logical_qubits)] == t.logical_qubits
+        assert sorted(t.layout) == list(range(12))
+        for q, i in t.global_to_local_map.items():
+            assert t.layout[i] == q
+
+
+def test_pass_manager_rewrites_in_schedule_order():
+    qc = BUILDERS["qft_swaps_n9_nL5"]()
+    pm, lqr = make_custom_pm(5)
+    tqc = pm.run(qc)
+    sched = lqr.property_set["flat_tiling_schedule"]
+    assert [ins.operation for ins in tqc.data] == [n.op for n in sched]
+    assert len(tqc.data) == len(qc.data)
+    summ = LazyQubitReordering.summarize_tiling(sched, lqr.property_set["flat_tiling_mapping"])
+    assert summ["num_tiles"] == len(lqr.property_set["flat_tiling_plan"])
+
+
+def test_empty_and_tiny():
+    from frontierlabproject_b200.circuit import QuantumCircuit
+    _, plan = tile_circuit(QuantumCircuit(3), 2)
+    assert plan == []
+    qc = QuantumCircuit(1)
+    qc.h(0)
+    _, plan = tile_circuit(qc, 4)
+    assert len(plan) == 1 and plan[0].layout == [0]
