@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark of the statevector tile executor.
+
+Workload (one step): the seeded random circuit n=30, depth 100 (per layer one gate per
+qubit from {H, X, SX, RX, RZ}, then CX on a random perfect matching), complex64, run from
+|0...0> along the reference LQR tile schedule at nL=20, ending with the state in the last
+tile's layout (the reference executor's output).
+
+Metric: algorithmic HBM throughput of a circuit, B_alg / t, with
+B_alg = (tiles + reorders + 1) * 2 * 2^n * 8 bytes (one read+write sweep of the state per
+tile, per reorder and for the final read-out, as the reference schedule executes it).
+``circuit_time_s`` is t itself.  ``value`` is device-timed (CUDA events on the executor's
+stream, inputs resident); ``e2e`` is the same metric through ``run_custom_backend`` with a
+pinned host result (8 GiB device->host per step) and the host-side op preparation.
+
+``--impl reference`` times the CPU implementation of the reference algorithm (one
+full-state pass per gate, out-of-place scatter per reorder; the C/OpenMP restatement in
+oracle/) on a bounded sample of the same workload and extrapolates to the whole schedule.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "n=30 circuit time & HBM GB/s vs peak; adjoint gradients/s at ≤1e-5 rel err"
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for nm, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(n, depth, nl, seed):
+    from frontierlabproject_b200 import circuits as C
+    from frontierlabproject_b200.transpiler import tile_circuit
+    qc = C.random_layered(n, depth, seed)
+    _, plan = tile_circuit(qc, nl)
+    layouts = [list(range(n))] + [list(t.layout) for t in plan]
+    reorders = sum(1 for a, b in zip(layouts[:-1], layouts[1:]) if a != b)
+    return qc, plan, reorders
+
+
+def prepared_tiles(qc, plan, np_dtype):
+    """Per tile: (layout, fused op batch) -- the executor inputs, built once."""
+    from frontierlabproject_b200.backend import fuse_tile_ops, tile_ops_for
+    from frontierlabproject_b200.qgpusim_cuda import _OpBatch
+    qmap = {q: qc.find_bit(q).index for q in qc.qubits}
+    code = 0 if np_dtype == np.complex64 else 1
+    out = []
+    for t in plan:
+        ops = fuse_tile_ops(tile_ops_for(t, qmap, np_dtype))
+        out.append((list(t.layout), _OpBatch(ops, code) if ops else None))
+    return out
+
+
+def traffic_from_profile():
+    """DRAM bytes per pass-kernel launch recorded from an ncu capture (profiles/)."""
+    p = os.path.join(HERE, "profiles", "pass_kernel_random_n30.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_sweep:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def cpu_reference_sample(qc, plan, n_cpu: int, budget_s: float):
+    """Time the C/OpenMP restatement of the reference kernels on a bounded sample of the
+    schedule (leading fused ops and reorders) and extrapolate to the whole schedule."""
+    import ctypes
+    from oracle import build as ob
+    from frontierlabproject_b200.backend import fuse_tile_ops, tile_ops_for
+    lib = ctypes.CDLL(ob.build())
+    lib.qo_apply_1q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.qo_apply_2q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    lib.qo_permute_scatter_c64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.qo_max_threads.restype = ctypes.c_int
+    threads = lib.qo_max_threads()
+    qmap = {q: qc.find_bit(q).index for q in qc.qubits}
+    n = qc.num_qubits
+    fused = []
+    for t in plan:
+        fused.extend(fuse_tile_ops(tile_ops_for(t, qmap, np.complex64)))
+    G = len(fused)
+    psi = np.zeros(1 << n_cpu, dtype=np.complex64)
+    psi[0] = 1
+    tmp = np.empty_like(psi)
+    t_gate = []
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < budget_s * 0.8 and k < len(fused):
+        op = fused[k]
+        U = np.ascontiguousarray(op[-1], np.complex64)
+        q0 = min(op[1], n_cpu - 1)
+        s = time.perf_counter()
+        if op[0] == "1q":
+            lib.qo_apply_1q_c64(psi.ctypes.data, n_cpu, q0, U.ctypes.data)
+        else:
+            q1 = min(op[2], n_cpu - 1)
+            if q1 == q0:
+                q1 = (q0 + 1) % n_cpu
+            lib.qo_apply_2q_c64(psi.ctypes.data, n_cpu, q0, q1, U.ctypes.data)
+        t_gate.append(time.perf_counter() - s)
+        k += 1
+    mp = np.random.default_rng(0).permutation(n_cpu).astype(np.int32)
+    s = time.perf_counter()
+    lib.qo_permute_scatter_c64(psi.ctypes.data, tmp.ctypes.data, n_cpu, mp.ctypes.data)
+    t_perm = time.perf_counter() - s
+    scale = float(1 << (n - n_cpu))
+    layouts = [list(range(n))] + [list(t.layout) for t in plan]
+    R = sum(1 for a, b in zip(layouts[:-1], layouts[1:]) if a != b)
+    t_total = (np.mean(t_gate) * G + t_perm * R) * scale
+    sample = (f"{len(t_gate)} leading fused gate passes + 1 reorder of the schedule at n={n_cpu}, "
+              f"extrapolated to {G} gate passes + {R} reorders" + (f" and scaled by 2^{n - n_cpu}" if n_cpu != n else ""))
+    return t_total, threads, sample
+
+
+def run_reference_arm(args, rank):
+    qc, plan, R = build_workload(args.n, args.depth, args.nl, args.seed)
+    n_cpu = choose_cpu_n(args.n)
+    sweep = 2 * (1 << args.n) * 8
+    b_alg = (len(plan) + R + 1) * sweep
+    times = []
+    threads, sample = None, None
+    for i in range(args.warmup + args.steps):
+        t, threads, sample = cpu_reference_sample(qc, plan, n_cpu, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            times.append(t)
+    t = float(np.mean(times))
+    v = b_alg / t / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "circuit_time_s": t,
+            "config": config_of(args, plan, R),
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def choose_cpu_n(n: int) -> int:
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 16 << 30
+    m = n
+    while m > 20 and 2 * (1 << m) * 8 > avail * 0.6:
+        m -= 1
+    return m
+
+
+def config_of(args, plan, R):
+    return {"workload": f"random circuit n={args.n} depth={args.depth} complex64 from |0>, reference LQR "
+                        f"schedule nL={args.nl} ({len(plan)} tiles, {R} reorders), seed {args.seed}",
+            "n": args.n, "depth": args.depth, "nL": args.nl, "tile_mode": args.mode,
+            "l2": "state (8 GiB at n=30) > L2 (126 MB): every sweep streams from HBM, no flush needed"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="graphed", choices=["graphed", "cooperative", "sequential"])
+    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=100)
+    ap.add_argument("--nl", type=int, default=20)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from frontierlabproject_b200 import build as B
+    B.build()
+    from frontierlabproject_b200.backend import run_custom_backend
+    from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
+
+    hbm_peak, peak_kind = peaks()
+    qc, plan, R = build_workload(args.n, args.depth, args.nl, args.seed)
+    tiles = prepared_tiles(qc, plan, np.complex64)
+    n = args.n
+    sweep = 2 * (1 << n) * 8
+    b_alg = (len(plan) + R + 1) * sweep
+
+    sv = StatevectorF32(n)
+    stream = torch.cuda.ExternalStream(sv.stream)
+    apply = {"graphed": sv.apply_tile_graphed, "cooperative": sv.apply_tile_cooperative,
+             "sequential": sv.apply_tile_dev}[args.mode]
+
+    def step(ev):
+        sv.reset()
+        ev[0].record(stream)
+        layout = list(range(n))
+        for lay, batch in tiles:
+            if lay != layout:
+                sv.permute(layout, lay)
+                layout = lay
+            if batch is not None:
+                apply(batch)
+        sv.materialize()
+        ev[1].record(stream)
+
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(args.warmup):
+        step(mk())
+    sv.synchronize()
+    sv.reset_stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    evs = [mk() for _ in range(args.steps)]
+    start.record(stream)
+    for i in range(args.steps):
+        step(evs[i])
+    end.record(stream)
+    sv.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = start.elapsed_time(end)
+    pass_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+    st = sv.stats()
+    if dist:
+        t = torch.tensor([total_ms, pass_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, pass_ms = t.tolist()
+    ms_step = total_ms / args.steps
+    value = b_alg * world / (ms_step / 1e3) / 1e9
+    sweeps_step = (st["sweeps"] + st["gate_sweeps"]) / args.steps
+    achieved = sweeps_step * sweep / (pass_ms / args.steps / 1e3) / 1e9
+    traffic = traffic_from_profile()
+    launches_step = 1 + (st["sweeps"] - st["perm_sweeps"]) / args.steps + (1 if st["perm_sweeps"] else 0) \
+        if args.mode == "graphed" else 1 + st["launches"] / args.steps
+
+    # ---- end to end through the public API (pinned host result) ----
+    e2e = None
+    if args.e2e_steps > 0:
+        out = torch.empty(1 << n, dtype=torch.complex64, pin_memory=True).numpy()
+        run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode=args.mode, sv=sv, out=out)
+        ts = []
+        for _ in range(args.e2e_steps):
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            _, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode=args.mode, sv=sv,
+                                        out=out)
+            ts.append(time.perf_counter() - t0)
+        te = float(np.mean(ts))
+        if dist:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = t.item()
+        h2d = sum(b.arr.nbytes + sum(k.nbytes for k in b._keep) for _, b in tiles if b is not None)
+        e2e = {"value": b_alg * world / te / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int((1 << n) * 8), "circuit_time_s": te}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        t_cpu, threads, sample = cpu_reference_sample(qc, plan, choose_cpu_n(n), args.cpu_budget)
+        cpu = {"value": b_alg / t_cpu / 1e9, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
+               "circuit_time_s": t_cpu}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "circuit_time_s": ms_step / 1e3,
+                "config": dict(config_of(args, plan, R), parallelism="replicas" if world > 1 else "single GPU"),
+                "sweeps_per_step": sweeps_step, "reference_sweeps_per_step": len(plan) + R + 1,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": achieved / hbm_peak, "traffic": traffic,
+                             "kernel": "pass_kernel<float,5>", "peak_kind": peak_kind,
+                             "algorithmic_bytes_per_sweep": sweep},
+                "gpu_launches": int(round(launches_step * args.steps)),
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

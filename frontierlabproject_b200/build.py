@@ -19,7 +19,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqsim_b200.so")
-SOURCES = ["kern_pass.cu", "kern_gate.cu", "state.cu", "plan.cpp"]
+SOURCES = ["kern_pass.cu", "kern_gate.cu", "state.cu", "plan.cpp", "jit.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -64,7 +64,8 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
             sys.stderr.write(log)
     objs = [o for o, _ in results]
     tmp = LIB + ".tmp"
-    cmd = [cc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-cudart", "static"]
+    cmd = [cc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC", "-cudart", "static", "-ldl",
+                                                        "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -1,0 +1,484 @@
+// Plan-time specialisation of pass kernels (see jit.h).
+#include "jit.h"
+
+#include <cuda.h>
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <list>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <thread>
+#include <unordered_map>
+
+namespace qsb {
+
+namespace {
+
+// ---- NVRTC (dlopen: the library is optional at load time) ---------------------------
+struct Nvrtc {
+  void* h = nullptr;
+  int (*create)(void**, const char*, const char*, int, const char* const*, const char* const*) = nullptr;
+  int (*compile)(void*, int, const char* const*) = nullptr;
+  int (*cubin_size)(void*, size_t*) = nullptr;
+  int (*cubin)(void*, char*) = nullptr;
+  int (*log_size)(void*, size_t*) = nullptr;
+  int (*log)(void*, char*) = nullptr;
+  int (*destroy)(void**) = nullptr;
+  std::string why;
+  bool ok = false;
+  Nvrtc() {
+    const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"};
+    for (const char* n : names) {
+      h = dlopen(n, RTLD_NOW | RTLD_LOCAL);
+      if (h) break;
+    }
+    if (!h) { why = "NVRTC (libnvrtc.so.12) not found"; return; }
+    create = (decltype(create))dlsym(h, "nvrtcCreateProgram");
+    compile = (decltype(compile))dlsym(h, "nvrtcCompileProgram");
+    cubin_size = (decltype(cubin_size))dlsym(h, "nvrtcGetCUBINSize");
+    cubin = (decltype(cubin))dlsym(h, "nvrtcGetCUBIN");
+    log_size = (decltype(log_size))dlsym(h, "nvrtcGetProgramLogSize");
+    log = (decltype(log))dlsym(h, "nvrtcGetProgramLog");
+    destroy = (decltype(destroy))dlsym(h, "nvrtcDestroyProgram");
+    ok = create && compile && cubin_size && cubin && log_size && log && destroy;
+    if (!ok) why = "NVRTC symbols missing";
+  }
+};
+
+Nvrtc& nvrtc() {
+  static Nvrtc n;
+  return n;
+}
+
+// ---- driver entry points through the runtime (no link-time libcuda dependency) -------
+struct Driver {
+  CUresult (*load)(CUmodule*, const void*) = nullptr;
+  CUresult (*unload)(CUmodule) = nullptr;
+  CUresult (*get_fn)(CUfunction*, CUmodule, const char*) = nullptr;
+  CUresult (*set_attr)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                     void**, void**) = nullptr;
+  bool ok = false;
+  std::string why;
+  Driver() {
+    auto get = [&](const char* name, void** fp) {
+      cudaDriverEntryPointQueryResult q;
+      cudaError_t e = cudaGetDriverEntryPointByVersion(name, fp, 12000, cudaEnableDefault, &q);
+      return e == cudaSuccess && q == cudaDriverEntryPointSuccess && *fp;
+    };
+    ok = get("cuModuleLoadData", (void**)&load) && get("cuModuleUnload", (void**)&unload) &&
+         get("cuModuleGetFunction", (void**)&get_fn) && get("cuFuncSetAttribute", (void**)&set_attr) &&
+         get("cuLaunchKernel", (void**)&launch);
+    if (!ok) why = "CUDA driver entry points unavailable";
+  }
+};
+
+Driver& driver() {
+  static Driver d;
+  return d;
+}
+
+std::string csrc_dir() {
+  Dl_info info;
+  if (dladdr((void*)&jit_available, &info) && info.dli_fname) {
+    std::string p(info.dli_fname);
+    size_t s = p.rfind('/');
+    return (s == std::string::npos ? std::string(".") : p.substr(0, s)) + "/csrc";
+  }
+  return "csrc";
+}
+
+int cls_of(float re, float im) {
+  if (re == 0.0f && im == 0.0f) return 0;
+  if (im == 0.0f) return re == 1.0f ? 1 : (re == -1.0f ? 2 : 5);
+  if (re == 0.0f) return im == 1.0f ? 3 : (im == -1.0f ? 4 : 6);
+  return 7;
+}
+
+uint64_t fnv(uint64_t h, const void* p, size_t n) {
+  const uint8_t* b = (const uint8_t*)p;
+  for (size_t i = 0; i < n; ++i) { h ^= b[i]; h *= 1099511628211ull; }
+  return h;
+}
+
+// ---- code generation ------------------------------------------------------------------
+struct Ent {
+  int cls = 0;          // 0 zero, 1 one, 2 minus one, 3 +i, 4 -i, 5 real, 6 imaginary, 7 general
+  std::string var;      // coefficient variable for classes 5..7
+};
+
+struct Gen {
+  std::ostringstream o;
+  const float* coef = nullptr;  // interleaved complex64 table
+  int nvar = 0;
+
+  Ent coef_ent(int off) {
+    Ent e;
+    e.cls = cls_of(coef[2 * off], coef[2 * off + 1]);
+    if (e.cls >= 5) {
+      e.var = "k" + std::to_string(nvar++);
+      o << "const float2 " << e.var << " = LK(" << off << ");";
+    }
+    return e;
+  }
+  static Ent cst(int cls) { Ent e; e.cls = cls; return e; }
+
+  // linear combination sum_c row[c] * x_c; empty string when all terms vanish
+  static std::string lin(const Ent* row, const char* const* x, int n) {
+    std::string re, im;
+    int nz = 0, last = -1;
+    for (int c = 0; c < n; ++c) {
+      const Ent& e = row[c];
+      const std::string X(x[c]);
+      const std::string& k = e.var;
+      switch (e.cls) {
+        case 0: continue;
+        case 1: re += "+" + X + ".x"; im += "+" + X + ".y"; break;
+        case 2: re += "-" + X + ".x"; im += "-" + X + ".y"; break;
+        case 3: re += "-" + X + ".y"; im += "+" + X + ".x"; break;
+        case 4: re += "+" + X + ".y"; im += "-" + X + ".x"; break;
+        case 5: re += "+" + k + ".x*" + X + ".x"; im += "+" + k + ".x*" + X + ".y"; break;
+        case 6: re += "-" + k + ".y*" + X + ".y"; im += "+" + k + ".y*" + X + ".x"; break;
+        default:
+          re += "+" + k + ".x*" + X + ".x-" + k + ".y*" + X + ".y";
+          im += "+" + k + ".x*" + X + ".y+" + k + ".y*" + X + ".x";
+      }
+      ++nz;
+      last = c;
+    }
+    if (nz == 0) return "make_float2(0.f,0.f)";
+    if (nz == 1 && row[last].cls == 1) return x[last];
+    return "make_float2(" + re + "," + im + ")";
+  }
+
+  static bool is_identity(const Ent* m, int d) {
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c)
+        if (m[r * d + c].cls != (r == c ? 1 : 0)) return false;
+    return true;
+  }
+
+  // 2x2 on register bit J
+  void pairs(int J, const Ent* m) {
+    if (is_identity(m, 2)) return;
+    static const char* x[2] = {"x0", "x1"};
+    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
+      << (1 << J) << "];a[i]=" << lin(m, x, 2) << ";a[i|" << (1 << J) << "]=" << lin(m + 2, x, 2) << ";}\n";
+  }
+  // 2x2 on register bit J, applied where the runtime condition holds (selects, no divergence)
+  void pairs_sel(int J, const Ent* m, const std::string& cond) {
+    if (is_identity(m, 2)) return;
+    static const char* x[2] = {"x0", "x1"};
+    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
+      << (1 << J) << "];const float2 y0=" << lin(m, x, 2) << ",y1=" << lin(m + 2, x, 2) << ";a[i]=(" << cond
+      << ")?y0:x0;a[i|" << (1 << J) << "]=(" << cond << ")?y1:x1;}\n";
+  }
+  // 4x4 on register bits (JA = matrix bit 0, JB = matrix bit 1)
+  void quads(int JA, int JB, const Ent* m) {
+    if (is_identity(m, 4)) return;
+    static const char* x[4] = {"x0", "x1", "x2", "x3"};
+    const int A = 1 << JA, B = 1 << JB;
+    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (A | B) << ")){const float2 x0=a[i],x1=a[i|" << A
+      << "],x2=a[i|" << B << "],x3=a[i|" << (A | B) << "];";
+    o << "a[i]=" << lin(m, x, 4) << ";a[i|" << A << "]=" << lin(m + 4, x, 4) << ";a[i|" << B
+      << "]=" << lin(m + 8, x, 4) << ";a[i|" << (A | B) << "]=" << lin(m + 12, x, 4) << ";}\n";
+  }
+  // every amplitude times a (possibly selected) scalar
+  void scale(const Ent& d) {
+    if (d.cls == 1) return;
+    static const char* x[1] = {"x0"};
+    o << "\n#pragma unroll\nfor(int i=0;i<32;++i){const float2 x0=a[i];a[i]=" << lin(&d, x, 1) << ";}\n";
+  }
+};
+
+std::string bitcond(int phys) { return "((pb>>" + std::to_string(phys) + ")&1ull)"; }
+
+void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& ph) {
+  auto& o = G.o;
+  o << "{";
+  const bool fa = g.a >= kFixed, fb = g.b >= kFixed;
+  const int c = g.coef;
+  // whether a fixed bit is uniform across the warp (group bit or warp-index bit)
+  auto warp_uniform = [&](int phys) {
+    for (int j = 0; j < 5 && j < pd.m - pd.r; ++j)
+      if (pd.sbit[ph.tbit[j]] == phys) return false;
+    return true;
+  };
+  switch (g.kind) {
+    case GK_1Q_DENSE: case GK_1Q_REAL: case GK_1Q_REIM: {
+      Ent m[4] = {G.coef_ent(c), G.coef_ent(c + 1), G.coef_ent(c + 2), G.coef_ent(c + 3)};
+      G.pairs(g.a, m);
+      break;
+    }
+    case GK_1Q_X: {
+      Ent m[4] = {Gen::cst(0), Gen::cst(1), Gen::cst(1), Gen::cst(0)};
+      G.pairs(g.a, m);
+      break;
+    }
+    case GK_1Q_DIAG: {
+      if (!fa) {
+        Ent m[4] = {G.coef_ent(c), Gen::cst(0), Gen::cst(0), G.coef_ent(c + 1)};
+        G.pairs(g.a, m);
+      } else {
+        o << "const float2 d=" << bitcond(g.a - kFixed) << "?LK(" << c + 1 << "):LK(" << c << ");";
+        Ent d;
+        d.cls = 7;
+        d.var = "d";
+        G.scale(d);
+      }
+      break;
+    }
+    case GK_2Q_DENSE: {
+      Ent m[16];
+      for (int e = 0; e < 16; ++e) m[e] = G.coef_ent(c + e);
+      G.quads(g.a, g.b, m);
+      break;
+    }
+    case GK_2Q_SWAP: {
+      Ent m[16];
+      const int P[4] = {0, 2, 1, 3};
+      for (int r = 0; r < 4; ++r)
+        for (int col = 0; col < 4; ++col) m[4 * r + col] = Gen::cst(col == P[r] ? 1 : 0);
+      G.quads(g.a, g.b, m);
+      break;
+    }
+    case GK_2Q_DIAG: {
+      if (!fa && !fb) {
+        Ent m[16];
+        for (int e = 0; e < 16; ++e) m[e] = Gen::cst(0);
+        for (int e = 0; e < 4; ++e) m[5 * e] = G.coef_ent(c + e);
+        G.quads(g.a, g.b, m);
+      } else if (fa && fb) {
+        o << "const int v=(int)" << bitcond(g.a - kFixed) << "+2*(int)" << bitcond(g.b - kFixed)
+          << ";const float2 d=LK(" << c << "+v);";
+        Ent d;
+        d.cls = 7;
+        d.var = "d";
+        G.scale(d);
+      } else {
+        // one fixed bit selects a diagonal 2x2 on the register bit
+        const int J = fa ? g.b : g.a;
+        const std::string cond = bitcond((fa ? g.a : g.b) - kFixed);
+        // entries indexed b_a + 2 b_b
+        const int lo0 = fa ? c + 0 : c + 0, hi0 = fa ? c + 2 : c + 1;   // fixed bit = 0
+        const int lo1 = fa ? c + 1 : c + 2, hi1 = fa ? c + 3 : c + 3;   // fixed bit = 1
+        o << "const float2 d0=" << cond << "?LK(" << lo1 << "):LK(" << lo0 << ");const float2 d1=" << cond
+          << "?LK(" << hi1 << "):LK(" << hi0 << ");";
+        Ent m[4];
+        m[0].cls = 7; m[0].var = "d0";
+        m[3].cls = 7; m[3].var = "d1";
+        G.pairs(J, m);
+      }
+      break;
+    }
+    case GK_2Q_CX: case GK_2Q_CU: {
+      Ent u[4];
+      if (g.kind == GK_2Q_CX) {
+        u[0] = Gen::cst(0); u[1] = Gen::cst(1); u[2] = Gen::cst(1); u[3] = Gen::cst(0);
+      } else {
+        for (int e = 0; e < 4; ++e) u[e] = G.coef_ent(c + e);
+      }
+      if (!fa) {
+        // control a (matrix bit 0), target b (matrix bit 1): U acts on indices 1 and 3
+        Ent m[16];
+        for (int r = 0; r < 4; ++r)
+          for (int col = 0; col < 4; ++col) m[4 * r + col] = Gen::cst((r == col && !(r & 1)) ? 1 : 0);
+        m[4 * 1 + 1] = u[0]; m[4 * 1 + 3] = u[1]; m[4 * 3 + 1] = u[2]; m[4 * 3 + 3] = u[3];
+        G.quads(g.a, g.b, m);
+      } else {
+        const int P = g.a - kFixed;
+        if (warp_uniform(P)) {
+          o << "if(" << bitcond(P) << "){";
+          G.pairs(g.b, u);
+          o << "}";
+        } else {
+          G.pairs_sel(g.b, u, bitcond(P));
+        }
+      }
+      break;
+    }
+    default:
+      throw std::runtime_error("jit: unknown gate kind " + std::to_string((int)g.kind));
+  }
+  o << "}\n";
+}
+
+const char* kPrelude = R"(
+#include "pass_body.cuh"
+__device__ __forceinline__ float2 ldk_(const float2* p) {
+  float2 v;
+  asm volatile("ld.global.nc.v2.f32 {%0,%1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+#define LK(i) ldk_(K + (i))
+)";
+
+}  // namespace
+
+JitKernels::~JitKernels() {
+  Driver& d = driver();
+  if (d.ok)
+    for (void* m : modules) d.unload((CUmodule)m);
+}
+
+bool jit_available(std::string* why) {
+  if (!nvrtc().ok) { if (why) *why = nvrtc().why; return false; }
+  if (!driver().ok) { if (why) *why = driver().why; return false; }
+  return true;
+}
+
+uint64_t jit_key(const Program& prog) {
+  const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
+  const float* cf = (const float*)(prog.bytes.data() + hdr->off_coef);
+  uint64_t h = fnv(1469598103934665603ull, prog.bytes.data(), hdr->off_coef);
+  std::vector<uint8_t> cls(hdr->ncoef);
+  for (int i = 0; i < hdr->ncoef; ++i) cls[i] = (uint8_t)cls_of(cf[2 * i], cf[2 * i + 1]);
+  return fnv(h, cls.data(), cls.size());
+}
+
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key) {
+  const uint8_t* b = prog.bytes.data();
+  const ProgramHeader* hdr = (const ProgramHeader*)b;
+  if (hdr->dtype != 0) throw std::runtime_error("jit: complex64 programs only");
+  const PassDesc* pds = (const PassDesc*)(b + hdr->off_pass);
+  const PhaseDesc* phs = (const PhaseDesc*)(b + hdr->off_phase);
+  const GateInstr* gis = (const GateInstr*)(b + hdr->off_gate);
+  Gen G;
+  G.coef = (const float*)(b + hdr->off_coef);
+  G.o << kPrelude;
+  char kname[64];
+  for (int p = pass_begin; p < pass_end; ++p) {
+    const PassDesc& pd = pds[p];
+    G.o << "struct X" << p << "{template<typename C,int LR>__device__ __forceinline__ static void run("
+        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb){"
+        << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
+    for (int h = 0; h < pd.nphase; ++h) {
+      const PhaseDesc& ph = phs[pd.phase0 + h];
+      G.o << "case " << h << ":{\n";
+      for (int gi = 0; gi < ph.ngate; ++gi) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+      G.o << "}break;\n";
+    }
+    std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
+    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(256,1) " << kname
+        << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi){qsb::pass_body<float,5,X" << p
+        << ">(prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
+  }
+  return G.o.str();
+}
+
+namespace {
+
+bool compile_source(const std::string& src, std::vector<char>* cubin, std::string* log) {
+  Nvrtc& nv = nvrtc();
+  void* prog = nullptr;
+  if (nv.create(&prog, src.c_str(), "qsim_jit.cu", 0, nullptr, nullptr) != 0) {
+    if (log) *log = "nvrtcCreateProgram failed";
+    return false;
+  }
+  const std::string inc = "-I" + csrc_dir();
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", inc.c_str(),
+                        "--extra-device-vectorization", "-lineinfo"};
+  const int rc = nv.compile(prog, 6, opts);
+  size_t ls = 0;
+  nv.log_size(prog, &ls);
+  std::string lg(ls, '\0');
+  if (ls) nv.log(prog, &lg[0]);
+  if (log) *log = lg;
+  bool ok = rc == 0;
+  if (ok && cubin) {
+    size_t cs = 0;
+    nv.cubin_size(prog, &cs);
+    cubin->resize(cs);
+    nv.cubin(prog, cubin->data());
+  }
+  nv.destroy(&prog);
+  return ok;
+}
+
+std::mutex g_mu;
+std::list<std::shared_ptr<JitKernels>> g_cache;  // most recent first
+
+}  // namespace
+
+bool jit_compile_check(const Program& prog, std::string* log) {
+  std::string why;
+  if (!nvrtc().ok) { if (log) *log = nvrtc().why; return false; }
+  const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
+  return compile_source(jit_source(prog, 0, hdr->npass, jit_key(prog)), nullptr, log);
+}
+
+std::shared_ptr<JitKernels> jit_get(const Program& prog) {
+  std::string why;
+  if (!jit_available(&why)) throw std::runtime_error("jit: " + why);
+  const uint64_t key = jit_key(prog);
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
+      if ((*it)->key == key) {
+        auto k = *it;
+        g_cache.erase(it);
+        g_cache.push_front(k);
+        return k;
+      }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
+  const int npass = hdr->npass;
+  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nchunk = std::max(1, std::min<int>(npass, (int)std::min(hw, 32u)));
+  std::vector<std::vector<char>> cubins(nchunk);
+  std::vector<std::string> logs(nchunk);
+  std::vector<int> ok(nchunk, 0);
+  std::vector<std::pair<int, int>> range(nchunk);
+  for (int c = 0; c < nchunk; ++c) range[c] = {npass * c / nchunk, npass * (c + 1) / nchunk};
+  {
+    std::vector<std::thread> th;
+    for (int c = 0; c < nchunk; ++c)
+      th.emplace_back([&, c] {
+        try {
+          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key), &cubins[c], &logs[c]);
+        } catch (const std::exception& e) {
+          logs[c] = e.what();
+        }
+      });
+    for (auto& t : th) t.join();
+  }
+  for (int c = 0; c < nchunk; ++c)
+    if (!ok[c]) throw std::runtime_error("jit: NVRTC compilation failed:\n" + logs[c].substr(0, 4000));
+  auto k = std::make_shared<JitKernels>();
+  k->key = key;
+  Driver& d = driver();
+  char kname[64];
+  for (int c = 0; c < nchunk; ++c) {
+    CUmodule mod;
+    if (d.load(&mod, cubins[c].data()) != CUDA_SUCCESS) throw std::runtime_error("jit: cuModuleLoadData failed");
+    k->modules.push_back(mod);
+    for (int p = range[c].first; p < range[c].second; ++p) {
+      std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
+      CUfunction f;
+      if (d.get_fn(&f, mod, kname) != CUDA_SUCCESS) throw std::runtime_error("jit: kernel not found");
+      if (d.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 200 * 1024) != CUDA_SUCCESS)
+        throw std::runtime_error("jit: cannot raise the shared-memory limit");
+      k->functions.push_back(f);
+    }
+  }
+  k->compile_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cache.push_front(k);
+  while (g_cache.size() > 8) g_cache.pop_back();
+  return k;
+}
+
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads, size_t smem,
+                       int grid, cudaStream_t stream) {
+  void* args[] = {(void*)&d_prog, (void*)&psi};
+  CUresult r = driver().launch((CUfunction)k.functions[p], grid, 1, 1, threads, 1, 1, (unsigned)smem,
+                               (CUstream)stream, args, nullptr);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+}  // namespace qsb

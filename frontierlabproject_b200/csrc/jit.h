@@ -1,0 +1,45 @@
+// Pass kernels specialised at plan time: each pass's register phases become straight-line
+// CUDA (no per-gate dispatch; permutation gates are register renames; zero, +-1, real and
+// imaginary matrix entries skip their multiplies), compiled for sm_100a with NVRTC and
+// loaded as cubins.  Coefficient values stay in the program's table, so a circuit whose
+// parameters change reuses the compiled kernels (the cache key is the program structure
+// plus the zero/one/real/imaginary class of every matrix entry).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "plan.h"
+
+namespace qsb {
+
+struct JitKernels {
+  std::vector<void*> functions;  // CUfunction per pass
+  std::vector<void*> modules;    // CUmodule per compiled chunk
+  uint64_t key = 0;
+  double compile_seconds = 0.0;
+  ~JitKernels();
+};
+
+// True when NVRTC and the driver entry points are available (message otherwise).
+bool jit_available(std::string* why);
+
+// Cache key of a complex64 program (structure + entry classes).
+uint64_t jit_key(const Program& prog);
+
+// CUDA source of the specialised kernels for passes [pass_begin, pass_end).
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key);
+
+// Compile (cached) the kernels of every pass of a complex64 program.
+std::shared_ptr<JitKernels> jit_get(const Program& prog);
+
+// Launch the specialised kernel of pass p (one launch per pass, no grid barrier).
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads, size_t smem,
+                       int grid, cudaStream_t stream);
+
+// Compile a program's source on the host only (tests; returns the NVRTC log on failure).
+bool jit_compile_check(const Program& prog, std::string* log);
+
+}  // namespace qsb

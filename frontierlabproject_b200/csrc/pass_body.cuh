@@ -1,0 +1,261 @@
+// Device code of a pass (sweep), shared by the generic pass kernel (kern_pass.cu, nvcc)
+// and the specialised kernels generated at plan time (jit.cpp, NVRTC).
+//
+// Per group (one value of the group bits) a block of 256 threads:
+//   load   16-byte cp.async copies -> swizzled shared memory, double-buffered: the next
+//          group's copies are in flight while the current group is processed;
+//   phases each thread reads its 2^LR amplitudes (the phase's register bits) from shared
+//          memory, the Exec policy applies the phase's gates in registers, writes back;
+//   store  shared memory -> 16-byte coalesced global stores, optionally through a bit
+//          permutation of the local bits (in-place permutation passes).
+// Several passes in one launch (cooperative mode) are separated by a grid barrier whose
+// wait is bounded (error word set, kernel returns).
+#pragma once
+#include "qsim.h"
+
+namespace qsb {
+
+template <typename Real> struct V2;
+template <> struct V2<float> { using T = float2; };
+template <> struct V2<double> { using T = double2; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+// a*x + b*y
+template <typename C> __device__ __forceinline__ C cmac2(C a, C x, C b, C y) {
+  C r;
+  r.x = a.x * x.x - a.y * x.y + b.x * y.x - b.y * y.y;
+  r.y = a.x * x.y + a.y * x.x + b.x * y.y + b.y * y.x;
+  return r;
+}
+
+// Opaque to the optimiser: forces a value to be recomputed / a pointer to be re-read
+// instead of keeping derived values live across the gate code.
+__device__ __forceinline__ void opaque(uint32_t& x) { asm volatile("" : "+r"(x)); }
+__device__ __forceinline__ void opaque(uint64_t& x) { asm volatile("" : "+l"(x)); }
+template <typename T> __device__ __forceinline__ const T* opaque_ptr(const T* p) {
+  asm volatile("" : "+l"(p));
+  return p;
+}
+
+template <typename Real> __device__ __forceinline__ uint32_t swz(uint32_t l);
+template <> __device__ __forceinline__ uint32_t swz<float>(uint32_t l) { return swz64(l); }
+template <> __device__ __forceinline__ uint32_t swz<double>(uint32_t l) { return swz128(l); }
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bar[0] = arrivals, bar[1] = generation.  Returns false when the wait gave up (the
+// error word is set; every block then leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned* err, uint64_t limit_ns) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned* vgen = bar + 1;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t t0 = global_ns();
+      while (*vgen == gen) {
+        if (*(volatile unsigned*)err != 0u) { ok = 0; break; }
+        if (global_ns() - t0 > limit_ns) { atomicExch(err, (unsigned)DERR_BARRIER_TIMEOUT); ok = 0; break; }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// physical offset of the local index l (deposit of l's bits onto the staged bits)
+__device__ __forceinline__ uint64_t phys_of_local(uint32_t l, const int8_t* sbit, int m) {
+  uint64_t q = 0;
+  for (int j = 0; j < m; ++j) if ((l >> j) & 1u) q |= 1ull << sbit[j];
+  return q;
+}
+__device__ __forceinline__ uint64_t group_base(uint64_t g, const int8_t* gbit, int ng) {
+  uint64_t b = 0;
+  for (int j = 0; j < ng; ++j) if ((g >> j) & 1ull) b |= 1ull << gbit[j];
+  return b;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+constexpr int kPassThreads = 256;
+
+// Issue the asynchronous load of group g into the shared buffer `buf` (16-byte copies,
+// swizzled destinations).  Items: c64 -> two amplitudes (local bit 0 inside the vector),
+// c128 -> one amplitude.
+template <typename Real>
+__device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const typename V2<Real>::T* psi,
+                                               uint64_t g, const PassDesc& pd, const uint64_t* pv, int T, int V) {
+  constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
+  const unsigned t = threadIdx.x;
+  if ((int)t >= T) return;
+  const uint64_t gbase = group_base(g, pd.gbit, pd.ngbits);
+  const uint32_t lt = (uint32_t)t << kItemBits;
+  const uint64_t base = gbase | phys_of_local(lt, pd.sbit, pd.m);
+#pragma unroll
+  for (int v = 0; v < 16; ++v) {
+    if (v >= V) break;
+    const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << kItemBits);
+    cp_async16(buf + swz<Real>(l), psi + (base | pv[v]));
+  }
+}
+
+// Exec::run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
+// thread's registers a[] (pb = physical index of the thread's register-0 amplitude).
+template <typename Real, int LR, typename Exec>
+__device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi,
+                                          int pass_begin, int pass_end, unsigned* bar, unsigned* err,
+                                          uint64_t barrier_limit_ns) {
+  using C = typename V2<Real>::T;
+  constexpr int NR = 1 << LR;
+  constexpr bool kC64 = sizeof(Real) == 4;
+  constexpr int kItemBits = kC64 ? 1 : 0;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassDesc pd;
+  __shared__ uint64_t pv[16];     // physical offset of load/store item row v
+  __shared__ uint32_t sv[16];     // store-permutation source local offset of row v
+
+  const unsigned t = threadIdx.x;
+  const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
+
+  for (int p = pass_begin; p < pass_end; ++p) {
+    if (p > pass_begin) {
+      if (!grid_barrier(bar, err, barrier_limit_ns)) return;
+    }
+    if (t == 0) pd = reinterpret_cast<const PassDesc*>(prog + hdr->off_pass)[p];
+    __syncthreads();
+    const int m = pd.m;
+    const int T = 1 << (m - pd.r);                    // active threads of this pass
+    const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (16)
+    for (int v = (int)t; v < V; v += (int)blockDim.x) {
+      const uint32_t lv = ((uint32_t)v * (uint32_t)T) << kItemBits;
+      uint64_t q = 0;
+      uint32_t s = 0;
+      for (int j = 0; j < m; ++j)
+        if ((lv >> j) & 1u) {
+          q |= 1ull << pd.sbit[j];
+          if (pd.store_perm) s |= 1u << pd.store_src[j];
+        }
+      pv[v] = q;
+      sv[v] = s;
+    }
+    __syncthreads();
+    const uint64_t ngroups = 1ull << pd.ngbits;
+    const bool active = (int)t < T;
+    C* bufs[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + (1u << m)};
+
+    uint64_t g = blockIdx.x;
+    if (g < ngroups) prefetch_group<Real>(bufs[0], psi, g, pd, pv, T, V);
+    cp_async_commit();
+    for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
+      C* sm = bufs[it & 1];
+      const uint64_t gn = g + gridDim.x;
+      if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gn, pd, pv, T, V);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      // ---- phases ----
+      for (int h = 0; h < pd.nphase; ++h) {
+        if (active) {
+          const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+          uint32_t sb;
+          uint64_t pb;
+          {
+            uint32_t lb = 0;
+            pb = group_base(g, pd.gbit, pd.ngbits);
+            const int nt = m - pd.r;
+            for (int j = 0; j < nt; ++j)
+              if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
+            sb = swz<Real>(lb);
+          }
+          uint32_t B[LR];
+#pragma unroll
+          for (int j = 0; j < LR; ++j) B[j] = swz<Real>(1u << ph->rbit[j]);
+          C a[NR];
+#pragma unroll
+          for (int i = 0; i < NR; ++i) {
+            uint32_t s = sb;
+#pragma unroll
+            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B[j];
+            a[i] = sm[s];
+          }
+          Exec::template run<C, LR>(prog, ph, p, h, a, pb);
+          opaque(sb);
+#pragma unroll
+          for (int j = 0; j < LR; ++j) opaque(B[j]);
+#pragma unroll
+          for (int i = 0; i < NR; ++i) {
+            uint32_t s = sb;
+#pragma unroll
+            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B[j];
+            sm[s] = a[i];
+          }
+        }
+        __syncthreads();
+      }
+      // ---- store ----
+      if (active) {
+        const uint64_t gbase = group_base(g, pd.gbit, pd.ngbits);
+        const uint32_t lt = (uint32_t)t << kItemBits;
+        const uint64_t base = gbase | phys_of_local(lt, pd.sbit, m);
+        uint32_t stt = 0;
+        if (pd.store_perm)
+          for (int j = 0; j < m; ++j) if ((lt >> j) & 1u) stt |= 1u << pd.store_src[j];
+        if constexpr (kC64) {
+#pragma unroll
+          for (int v = 0; v < 16; ++v) {
+            if (v >= V) break;
+            float4 val;
+            if (pd.store_perm) {
+              const uint32_t s0 = stt | sv[v];
+              const uint32_t s1 = s0 ^ (1u << pd.store_src[0]);
+              const C x0 = sm[swz<Real>(s0)], x1 = sm[swz<Real>(s1)];
+              val = make_float4(x0.x, x0.y, x1.x, x1.y);
+            } else {
+              const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << 1);
+              val = *reinterpret_cast<const float4*>(sm + swz<Real>(l));
+            }
+            __stcg(reinterpret_cast<float4*>(psi + (base | pv[v])), val);
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < 16; ++v) {
+            if (v >= V) break;
+            const uint32_t l = lt | ((uint32_t)v * (uint32_t)T);
+            const uint32_t src = pd.store_perm ? (stt | sv[v]) : l;
+            __stcg(psi + (base | pv[v]), sm[swz<Real>(src)]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+}
+
+}  // namespace qsb

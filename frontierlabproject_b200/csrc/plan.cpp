@@ -455,6 +455,7 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
     for (size_t i = 0; i < coef.size(); ++i) { cf[2 * i] = coef[i].real(); cf[2 * i + 1] = coef[i].imag(); }
   }
   prog.structure_hash = h;
+  prog.has_gates = !gi.empty();
   prog.npass = (int)pd.size();
   prog.threads = threads;
   prog.max_smem = smem;

@@ -65,6 +65,7 @@ struct Program {
   int npass = 0;
   int threads = 0;        // block size (max over passes of 2^(m - r))
   size_t max_smem = 0;    // bytes of shared memory per block
+  bool has_gates = false;  // at least one gate instruction
 };
 
 Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops,
@@ -72,17 +73,5 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
 
 // Reference interpretation of a program on host memory (used by CPU tests of the planner).
 void emulate_program(const uint8_t* prog, void* state, int n, int dtype);
-
-// Bank-spreading swizzle of a local amplitude index inside the shared-memory group.
-// complex64: XOR bits 1..3 with a fold of bits 4.. (bit 0 kept so aligned pairs stay together);
-// complex128: XOR bits 0..2 with a fold of bits 3..
-__host__ __device__ inline uint32_t swz64(uint32_t l) {
-  uint32_t f = (l >> 4) ^ (l >> 7) ^ (l >> 10) ^ (l >> 13);
-  return l ^ ((f & 7u) << 1);
-}
-__host__ __device__ inline uint32_t swz128(uint32_t l) {
-  uint32_t f = (l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12);
-  return l ^ (f & 7u);
-}
 
 }  // namespace qsb

@@ -13,9 +13,19 @@
 //              (2^r amplitudes per thread); gates whose data bits are register bits run
 //              entirely in registers.  Diagonal gates and controls need no register bit.
 #pragma once
-#include <cstdint>
+#ifdef __CUDACC_RTC__
+// compiled by NVRTC (kernels generated at plan time): no standard headers
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#else
 #include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
+#endif
 
 namespace qsb {
 
@@ -84,5 +94,18 @@ enum DeviceError : uint32_t {
   DERR_BARRIER_TIMEOUT = 1,
   DERR_BAD_PROGRAM = 2,
 };
+
+// Bank-spreading swizzle of a local amplitude index inside the shared-memory group.
+// complex64: XOR bits 1..3 with a fold of bits 4.. (bit 0 kept so aligned pairs stay together);
+// complex128: XOR bits 0..2 with a fold of bits 3..  Both are XOR-linear, so
+// swz(a | b) = swz(a) ^ swz(b) for disjoint a, b.
+__host__ __device__ inline uint32_t swz64(uint32_t l) {
+  uint32_t f = (l >> 4) ^ (l >> 7) ^ (l >> 10) ^ (l >> 13);
+  return l ^ ((f & 7u) << 1);
+}
+__host__ __device__ inline uint32_t swz128(uint32_t l) {
+  uint32_t f = (l >> 3) ^ (l >> 6) ^ (l >> 9) ^ (l >> 12);
+  return l ^ (f & 7u);
+}
 
 }  // namespace qsb

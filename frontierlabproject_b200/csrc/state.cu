@@ -22,6 +22,7 @@
 
 #include "../../include/qsim_b200.h"
 #include "kernels.h"
+#include "jit.h"
 #include "plan.h"
 #include "qsim.h"
 
@@ -59,6 +60,7 @@ int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
   uint64_t key = 0;
+  std::shared_ptr<JitKernels> kernels;
 };
 
 struct qs_state {
@@ -74,27 +76,36 @@ struct qs_state {
   int queue_mode = QS_MODE_COOPERATIVE;
   PlanConfig cfg;
   int grid_mult = 0;
+  int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
   // device scratch: program buffer, control words (barrier x2, error), accumulators
   uint8_t* d_prog = nullptr;
   size_t prog_cap = 0;
-  uint8_t* h_prog = nullptr;  // pinned staging of the program
-  size_t hprog_cap = 0;
-  cudaEvent_t prog_copied = nullptr;
+  struct Slot {            // pinned staging of an encoded program
+    uint8_t* host = nullptr;
+    size_t cap = 0;
+    cudaEvent_t done = nullptr;
+  };
+  static constexpr int kSlots = 4;
+  Slot slots[kSlots];
+  int next_slot = 0;
   unsigned* d_ctl = nullptr;
   double* d_acc = nullptr;
   double* h_acc = nullptr;    // pinned
   GraphEntry graph;
+  std::vector<std::pair<uint64_t, std::pair<size_t, std::vector<PlannedPass>>>> plan_cache;
   qs_stats st{};
 
   ~qs_state() {
     if (graph.exec) cudaGraphExecDestroy(graph.exec);
     if (psi) cudaFree(psi);
     if (d_prog) cudaFree(d_prog);
-    if (h_prog) cudaFreeHost(h_prog);
+    for (Slot& s : slots) {
+      if (s.host) cudaFreeHost(s.host);
+      if (s.done) cudaEventDestroy(s.done);
+    }
     if (h_acc) cudaFreeHost(h_acc);
     if (d_ctl) cudaFree(d_ctl);
     if (d_acc) cudaFree(d_acc);
-    if (prog_copied) cudaEventDestroy(prog_copied);
     if (stream && own_stream) cudaStreamDestroy(stream);
   }
 
@@ -111,21 +122,26 @@ struct qs_state {
       CK(cudaMalloc(&d_prog, prog_cap));
       if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
     }
-    if (bytes > hprog_cap) {
-      CK(cudaEventSynchronize(prog_copied));
-      if (h_prog) CK(cudaFreeHost(h_prog));
-      hprog_cap = std::max<size_t>(bytes * 2, 1 << 16);
-      CK(cudaMallocHost(&h_prog, hprog_cap));
-    }
   }
 
-  // copy the encoded program to the device (ordered on the stream)
+  // Copy the encoded program to the device, ordered on the stream.  The pinned staging
+  // is a ring of slots so the host can prepare the next launches while earlier copies
+  // are still queued behind running kernels.
   void upload(const Program& prog) {
-    ensure_prog(prog.bytes.size());
-    CK(cudaEventSynchronize(prog_copied));  // previous upload finished reading h_prog
-    std::memcpy(h_prog, prog.bytes.data(), prog.bytes.size());
-    CK(cudaMemcpyAsync(d_prog, h_prog, prog.bytes.size(), cudaMemcpyHostToDevice, stream));
-    CK(cudaEventRecord(prog_copied, stream));
+    const size_t bytes = prog.bytes.size();
+    ensure_prog(bytes);
+    Slot& s = slots[next_slot];
+    next_slot = (next_slot + 1) % kSlots;
+    if (!s.done) CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    CK(cudaEventSynchronize(s.done));  // the copy that last used this slot has run
+    if (bytes > s.cap) {
+      if (s.host) CK(cudaFreeHost(s.host));
+      s.cap = std::max<size_t>(bytes * 2, 1 << 16);
+      CK(cudaMallocHost(&s.host, s.cap));
+    }
+    std::memcpy(s.host, prog.bytes.data(), bytes);
+    CK(cudaMemcpyAsync(d_prog, s.host, bytes, cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(s.done, stream));
   }
 
   int grid_for_program(const Program& prog) {
@@ -146,16 +162,26 @@ struct qs_state {
                             d_ctl + 2, kBarrierLimitNs, stream));
       st.launches += 1;
     } else {
-      const uint64_t key = prog.structure_hash ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
-                           ((uint64_t)(uintptr_t)d_prog << 1) ^ (uint64_t)grid;
+      // specialised kernels for large complex64 states (compiled once per structure)
+      std::shared_ptr<JitKernels> jk;
+      if (dtype == 0 && prog.has_gates && (jit_mode > 0 || (jit_mode == 0 && n >= 20))) {
+        std::string why;
+        if (jit_available(&why)) jk = jit_get(prog);
+        else if (jit_mode > 0) throw InvalidArg{"jit requested but unavailable: " + why};
+      }
+      const uint64_t skey = jk ? jk->key : prog.structure_hash;
+      const uint64_t key = skey ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
+                           ((uint64_t)(uintptr_t)d_prog << 1) ^ (uint64_t)grid ^ (jk ? 0x5bd1e995ull : 0ull);
       if (!graph.exec || graph.key != key) {
         if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
+        graph.kernels = jk;  // keep the modules alive while the graph exists
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int p = 0; p < prog.npass && e == cudaSuccess; ++p)
-          e = launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false, d_ctl,
-                                 d_ctl + 2, kBarrierLimitNs, stream);
+          e = jk ? jit_launch(*jk, p, d_prog, psi, prog.threads, prog.max_smem, grid, stream)
+                 : launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false,
+                                      d_ctl, d_ctl + 2, kBarrierLimitNs, stream);
         cudaError_t e2 = cudaStreamEndCapture(stream, &g);
         if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
         if (e2 != cudaSuccess) throw CudaError{e2};
@@ -204,8 +230,22 @@ struct qs_state {
     cops.reserve(ops.size());
     for (const QOp& o : ops) cops.push_back(classify(o));
     PlanConfig c = eff_cfg();
-    auto passes = plan_passes(cops, n, c);
-    Program prog = encode_program(passes, cops, n, dtype);
+    // The plan depends on the gate classes and bits only, not on the matrix values:
+    // repeated circuits (parameter sweeps, benchmark steps) reuse it.
+    uint64_t key = 1469598103934665603ull;
+    auto mix = [&key](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
+    mix((uint64_t)n); mix((uint64_t)dtype); mix((uint64_t)c.m); mix((uint64_t)c.k); mix((uint64_t)c.hill_iters);
+    for (const COp& o : cops) mix(((uint64_t)o.kind << 16) | ((uint64_t)(o.a & 0xff) << 8) | (uint64_t)(o.b & 0xff));
+    const std::vector<PlannedPass>* passes = nullptr;
+    for (auto& e : plan_cache)
+      if (e.first == key && e.second.first == cops.size()) { passes = &e.second.second; break; }
+    if (!passes) {
+      if (plan_cache.size() >= 4) plan_cache.erase(plan_cache.begin());
+      plan_cache.emplace_back(key, std::make_pair(cops.size(), plan_passes(cops, n, c)));
+      passes = &plan_cache.back().second.second;
+      st.plans += 1;
+    }
+    Program prog = encode_program(*passes, cops, n, dtype);
     run_program(prog, queue_mode);
   }
 
@@ -366,7 +406,6 @@ int qs_create(int num_qubits, int dtype, qs_state** out) {
     s->pos2bit.resize(num_qubits);
     for (int p = 0; p < num_qubits; ++p) s->pos2bit[p] = p;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&s->prog_copied, cudaEventDisableTiming));
     CK(cudaMalloc(&s->psi, s->dim * s->esz));
     CK(cudaMalloc(&s->d_ctl, 4 * sizeof(unsigned)));
     CK(cudaMalloc(&s->d_acc, 8 * sizeof(double)));
@@ -508,6 +547,10 @@ int qs_flush(qs_state* s) {
   return guard([&] { if (!s) throw InvalidArg{"null state"}; s->flush(); });
 }
 
+int qs_materialize(qs_state* s) {
+  return guard([&] { if (!s) throw InvalidArg{"null state"}; s->materialize(); });
+}
+
 int qs_device_ptr(qs_state* s, void** out) {
   return guard([&] {
     if (!s || !out) throw InvalidArg{"null argument"};
@@ -550,6 +593,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     s->cfg.k = c->k;
     s->cfg.hill_iters = c->hill_iters;
     s->grid_mult = c->grid_mult;
+    s->jit_mode = c->jit;
   });
 }
 
@@ -557,6 +601,7 @@ int qs_get_config(qs_state* s, qs_config* c) {
   return guard([&] {
     if (!s || !c) throw InvalidArg{"null argument"};
     c->m = s->cfg.m; c->k = s->cfg.k; c->hill_iters = s->cfg.hill_iters; c->grid_mult = s->grid_mult;
+    c->jit = s->jit_mode;
   });
 }
 
@@ -675,6 +720,20 @@ int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const
     auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
     Program prog = encode_program(passes, c, num_qubits, dtype);
     emulate_program(prog.bytes.data(), psi, num_qubits, dtype);
+  });
+}
+
+int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps) {
+  return guard([&] {
+    if (num_qubits < reg_bits(0) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
+    auto q = convert_ops(nullptr, ops, nops, num_qubits, 0, false);
+    std::vector<COp> c;
+    for (auto& o : q) c.push_back(classify(o));
+    auto passes = plan_passes(c, num_qubits, cfg_from(0, num_qubits, cfg));
+    Program prog = encode_program(passes, c, num_qubits, 0);
+    std::string log;
+    if (!jit_compile_check(prog, &log)) throw InvalidArg{"jit compile failed:\n" + log.substr(0, 4000)};
+    if (sweeps) *sweeps = prog.npass;
   });
 }
 

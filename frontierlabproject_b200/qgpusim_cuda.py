@@ -171,7 +171,12 @@ class _StatevectorBase:
         N.call("qs_synchronize", self._h)
 
     def flush(self) -> None:
+        """Launch queued ops now (asynchronous)."""
         N.call("qs_flush", self._h)
+
+    def materialize(self) -> None:
+        """Launch queued ops and the data movement to the current layout (asynchronous)."""
+        N.call("qs_materialize", self._h)
 
     # -- layout ------------------------------------------------------------------------
     def permute(self, layout_old: Sequence[int], layout_new: Sequence[int]) -> None:
@@ -243,9 +248,15 @@ class _StatevectorBase:
     def reset_stats(self) -> None:
         N.call("qs_reset_stats", self._h)
 
-    def set_config(self, m: int = None, k: int = None, hill_iters: int = None, grid_mult: int = None) -> None:
+    def set_config(self, m: int = None, k: int = None, hill_iters: int = None, grid_mult: int = None,
+                   jit: int = None) -> None:
+        """Executor knobs: staged bits per sweep ``m``, always-staged low bits ``k``, planner
+        effort ``hill_iters``, blocks per SM ``grid_mult``, specialised kernels ``jit``
+        (0 auto, 1 always, -1 never)."""
         c = N.QsConfig()
         N.call("qs_get_config", self._h, byref(c))
+        if jit is not None:
+            c.jit = jit
         if m is not None:
             c.m = m
         if k is not None:

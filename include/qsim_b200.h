@@ -60,6 +60,8 @@ typedef struct {
   int k;          /* lowest physical bits always staged (>= 1) */
   int hill_iters; /* planner search effort */
   int grid_mult;  /* resident blocks per SM used by the pass kernel (0 = occupancy) */
+  int jit;        /* plan-time specialised kernels in graphed mode: 0 auto (complex64,
+                     >= 20 qubits), 1 always (complex64), -1 never */
 } qs_config;
 
 typedef struct {
@@ -72,6 +74,7 @@ typedef struct {
   unsigned long long graph_builds;   /* graph captures */
   unsigned long long flushes;        /* planned executions */
   unsigned long long permutes;       /* permute() calls */
+  unsigned long long plans;          /* pass plans computed (cache misses) */
 } qs_stats;
 
 /* Library */
@@ -112,6 +115,8 @@ QS_API int qs_apply_diagonal_1q(qs_state* s, int target_qubit, const double* pha
 
 /* Run queued ops now (asynchronously on the state's stream). */
 QS_API int qs_flush(qs_state* s);
+/* Run queued ops and move the data to the current layout (asynchronously). */
+QS_API int qs_materialize(qs_state* s);
 /* Device address of the amplitudes in the current layout (executes queued ops and
  * pending data movement, then synchronises).  Valid until the next call on s. */
 QS_API int qs_device_ptr(qs_state* s, void** out);
@@ -145,6 +150,9 @@ QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, c
 /* Host emulation of the planned program (tests of the planner, no GPU needed):
  * applies ops to the host state psi (2^n entries, dtype precision). */
 QS_API int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg, void* psi);
+/* Generate and compile (NVRTC, sm_100a, host only) the specialised kernels of the planned
+ * program for ops; returns QS_ERR_INVALID with the compiler log on failure. */
+QS_API int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps);
 /* Host emulation of the in-place permutation program: perm[b] = destination bit. */
 QS_API int qs_perm_emulate(int num_qubits, int dtype, const int* perm, const qs_config* cfg, void* psi,
                     int* sweeps);

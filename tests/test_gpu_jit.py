@@ -1,0 +1,84 @@
+"""Plan-time specialised pass kernels (NVRTC, graphed mode, complex64) against the oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from frontierlabproject_b200 import _native as N
+from frontierlabproject_b200 import circuits as C
+from frontierlabproject_b200.backend import run_custom_backend
+from frontierlabproject_b200.qgpusim_cuda import StatevectorF32, _OpBatch
+from frontierlabproject_b200.transpiler import tile_circuit
+from oracle import statevector as O
+from tests.cases import BUILDERS, ops_of
+from tests.test_planner_cpu import _mixed
+
+
+def test_jit_source_compiles_for_sm100a(native_lib):
+    qc = _mixed(12, 3)
+    b = _OpBatch(ops_of(qc), 0)
+    sw = ctypes.c_int()
+    rc = native_lib.qs_jit_check(12, b.ptr, len(b), None, ctypes.byref(sw))
+    if rc != 0 and b"NVRTC" in native_lib.qs_last_error() and b"not found" in native_lib.qs_last_error():
+        pytest.skip("NVRTC unavailable")
+    assert rc == 0, native_lib.qs_last_error().decode()
+    assert sw.value >= 1
+
+
+def _run_jit(qc, nl, **kw):
+    _, plan = tile_circuit(qc, nl)
+    sv = StatevectorF32(qc.num_qubits)
+    sv.set_config(jit=1)
+    psi, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv, **kw)
+    return psi, met, plan, sv
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [9, 13, 16])
+def test_jit_mixed_gates(n):
+    qc = _mixed(n, n + 1)
+    psi, met, plan, sv = _run_jit(qc, max(4, n - 3), logical_order=True)
+    assert O.infidelity(O.simulate(qc), psi) <= 1e-5
+    assert np.max(np.abs(psi - O.simulate(qc))) <= 1e-5
+    assert sv.stats()["graph_builds"] >= 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["random_layered_n12_d8_s2_nL8", "qft_swaps_n9_nL5", "hea_n8_L3_nL5",
+                                  "reference_random_n10_d4_s42_nL6"])
+def test_jit_reference_executor_states(name, golden_states):
+    qc = BUILDERS[name]()
+    nl = int(name.split("_nL")[1].split("_")[0])
+    psi, _, _, _ = _run_jit(qc, nl)
+    assert O.infidelity(golden_states[name], psi) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_jit_config0_n20_and_replay():
+    # n=20 takes the specialised kernels by default; a second run replays the cached graph
+    qc = C.random_layered(20, 20, 0)
+    _, plan = tile_circuit(qc, 14)
+    ref, _ = O.run_tile_plan(qc, plan, np.complex128)
+    sv = StatevectorF32(20)
+    for _ in range(2):
+        psi, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv)
+        assert O.infidelity(ref, psi) <= 1e-5
+    st = sv.stats()
+    assert st["graph_replays"] >= 1
+
+
+@pytest.mark.gpu
+def test_jit_parameter_change_reuses_kernels():
+    # same structure, new angles: results follow the new angles (coefficients are data)
+    n, L = 14, 3
+    rng = np.random.default_rng(0)
+    sv = StatevectorF32(n)
+    sv.set_config(jit=1)
+    a, b = C.hea_observable(n, 1)
+    for trial in range(2):
+        th = rng.uniform(-np.pi, np.pi, 2 * n * L)
+        qc = C.hea_ansatz(n, L, th)
+        _, plan = tile_circuit(qc, 10)
+        psi, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv,
+                                    logical_order=True)
+        assert O.infidelity(O.simulate(qc), psi) <= 1e-5
