@@ -236,6 +236,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--jit", type=int, default=0, help="0 auto, 1 always, -1 never")
+    ap.add_argument("--jit-lr", type=int, default=4)
+    ap.add_argument("--jit-blocks", type=int, default=1)
+    ap.add_argument("--m", type=int, default=13)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -267,6 +271,7 @@ def main():
     b_alg = (len(plan) + R + 1) * sweep
 
     sv = StatevectorF32(n)
+    sv.set_config(m=args.m, jit=args.jit, jit_lr=args.jit_lr, jit_blocks=args.jit_blocks)
     stream = torch.cuda.ExternalStream(sv.stream)
     apply = {"graphed": sv.apply_tile_graphed, "cooperative": sv.apply_tile_cooperative,
              "sequential": sv.apply_tile_dev}[args.mode]

@@ -27,13 +27,14 @@ OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
 
 
 class QsConfig(ctypes.Structure):
-    _fields_ = [("m", c_int), ("k", c_int), ("hill_iters", c_int), ("grid_mult", c_int), ("jit", c_int)]
+    _fields_ = [("m", c_int), ("k", c_int), ("hill_iters", c_int), ("grid_mult", c_int), ("jit", c_int),
+                ("jit_lr", c_int), ("jit_blocks", c_int)]
 
 
 class QsStats(ctypes.Structure):
     _fields_ = [(name, c_ulonglong) for name in
                 ("gates", "sweeps", "perm_sweeps", "gate_sweeps", "launches", "graph_replays",
-                 "graph_builds", "flushes", "permutes", "plans")]
+                 "graph_builds", "flushes", "permutes", "plans", "jit_compile_ms")]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -75,7 +76,7 @@ _SIGS = {
     "qs_plan_info": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), POINTER(c_int)],
     "qs_plan_emulate": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), c_void_p],
     "qs_perm_emulate": [c_int, c_int, c_void_p, POINTER(QsConfig), c_void_p, POINTER(c_int)],
-    "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int)],
+    "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), c_void_p, c_int],
 }
 
 _lib = None

@@ -166,14 +166,14 @@ struct Gen {
   void pairs(int J, const Ent* m) {
     if (is_identity(m, 2)) return;
     static const char* x[2] = {"x0", "x1"};
-    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
       << (1 << J) << "];a[i]=" << lin(m, x, 2) << ";a[i|" << (1 << J) << "]=" << lin(m + 2, x, 2) << ";}\n";
   }
   // 2x2 on register bit J, applied where the runtime condition holds (selects, no divergence)
   void pairs_sel(int J, const Ent* m, const std::string& cond) {
     if (is_identity(m, 2)) return;
     static const char* x[2] = {"x0", "x1"};
-    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
       << (1 << J) << "];const float2 y0=" << lin(m, x, 2) << ",y1=" << lin(m + 2, x, 2) << ";a[i]=(" << cond
       << ")?y0:x0;a[i|" << (1 << J) << "]=(" << cond << ")?y1:x1;}\n";
   }
@@ -182,7 +182,7 @@ struct Gen {
     if (is_identity(m, 4)) return;
     static const char* x[4] = {"x0", "x1", "x2", "x3"};
     const int A = 1 << JA, B = 1 << JB;
-    o << "\n#pragma unroll\nfor(int i=0;i<32;++i) if(!(i&" << (A | B) << ")){const float2 x0=a[i],x1=a[i|" << A
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (A | B) << ")){const float2 x0=a[i],x1=a[i|" << A
       << "],x2=a[i|" << B << "],x3=a[i|" << (A | B) << "];";
     o << "a[i]=" << lin(m, x, 4) << ";a[i|" << A << "]=" << lin(m + 4, x, 4) << ";a[i|" << B
       << "]=" << lin(m + 8, x, 4) << ";a[i|" << (A | B) << "]=" << lin(m + 12, x, 4) << ";}\n";
@@ -191,7 +191,7 @@ struct Gen {
   void scale(const Ent& d) {
     if (d.cls == 1) return;
     static const char* x[1] = {"x0"};
-    o << "\n#pragma unroll\nfor(int i=0;i<32;++i){const float2 x0=a[i];a[i]=" << lin(&d, x, 1) << ";}\n";
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i){const float2 x0=a[i];a[i]=" << lin(&d, x, 1) << ";}\n";
   }
 };
 
@@ -331,16 +331,17 @@ bool jit_available(std::string* why) {
   return true;
 }
 
-uint64_t jit_key(const Program& prog) {
+uint64_t jit_key(const Program& prog, const JitConfig& cfg) {
   const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
   const float* cf = (const float*)(prog.bytes.data() + hdr->off_coef);
   uint64_t h = fnv(1469598103934665603ull, prog.bytes.data(), hdr->off_coef);
   std::vector<uint8_t> cls(hdr->ncoef);
   for (int i = 0; i < hdr->ncoef; ++i) cls[i] = (uint8_t)cls_of(cf[2 * i], cf[2 * i + 1]);
-  return fnv(h, cls.data(), cls.size());
+  h = fnv(h, cls.data(), cls.size());
+  return fnv(h, &cfg.blocks, sizeof(cfg.blocks));
 }
 
-std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key) {
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg) {
   const uint8_t* b = prog.bytes.data();
   const ProgramHeader* hdr = (const ProgramHeader*)b;
   if (hdr->dtype != 0) throw std::runtime_error("jit: complex64 programs only");
@@ -354,7 +355,7 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
   for (int p = pass_begin; p < pass_end; ++p) {
     const PassDesc& pd = pds[p];
     G.o << "struct X" << p << "{template<typename C,int LR>__device__ __forceinline__ static void run("
-        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb){"
+        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb){constexpr int NR=1<<LR;"
         << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     for (int h = 0; h < pd.nphase; ++h) {
       const PhaseDesc& ph = phs[pd.phase0 + h];
@@ -363,8 +364,10 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       G.o << "}break;\n";
     }
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
-    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(256,1) " << kname
-        << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi){qsb::pass_body<float,5,X" << p
+    // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block
+    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(" << (1 << (pd.m - pd.r)) << ","
+        << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi)"
+        << "{qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
         << ">(prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
   }
   return G.o.str();
@@ -372,7 +375,7 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
 
 namespace {
 
-bool compile_source(const std::string& src, std::vector<char>* cubin, std::string* log) {
+bool compile_source(const std::string& src, std::vector<char>* cubin, std::string* log, bool verbose = false) {
   Nvrtc& nv = nvrtc();
   void* prog = nullptr;
   if (nv.create(&prog, src.c_str(), "qsim_jit.cu", 0, nullptr, nullptr) != 0) {
@@ -381,8 +384,8 @@ bool compile_source(const std::string& src, std::vector<char>* cubin, std::strin
   }
   const std::string inc = "-I" + csrc_dir();
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", inc.c_str(),
-                        "--extra-device-vectorization", "-lineinfo"};
-  const int rc = nv.compile(prog, 6, opts);
+                        "--extra-device-vectorization", "-lineinfo", "--ptxas-options=-v"};
+  const int rc = nv.compile(prog, verbose ? 7 : 6, opts);
   size_t ls = 0;
   nv.log_size(prog, &ls);
   std::string lg(ls, '\0');
@@ -408,13 +411,14 @@ bool jit_compile_check(const Program& prog, std::string* log) {
   std::string why;
   if (!nvrtc().ok) { if (log) *log = nvrtc().why; return false; }
   const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
-  return compile_source(jit_source(prog, 0, hdr->npass, jit_key(prog)), nullptr, log);
+  const JitConfig cfg;
+  return compile_source(jit_source(prog, 0, hdr->npass, jit_key(prog, cfg), cfg), nullptr, log, true);
 }
 
-std::shared_ptr<JitKernels> jit_get(const Program& prog) {
+std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
   std::string why;
   if (!jit_available(&why)) throw std::runtime_error("jit: " + why);
-  const uint64_t key = jit_key(prog);
+  const uint64_t key = jit_key(prog, cfg);
   {
     std::lock_guard<std::mutex> lk(g_mu);
     for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
@@ -440,7 +444,7 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog) {
     for (int c = 0; c < nchunk; ++c)
       th.emplace_back([&, c] {
         try {
-          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key), &cubins[c], &logs[c]);
+          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key, cfg), &cubins[c], &logs[c]);
         } catch (const std::exception& e) {
           logs[c] = e.what();
         }
@@ -451,6 +455,7 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog) {
     if (!ok[c]) throw std::runtime_error("jit: NVRTC compilation failed:\n" + logs[c].substr(0, 4000));
   auto k = std::make_shared<JitKernels>();
   k->key = key;
+  k->blocks = cfg.blocks;
   Driver& d = driver();
   char kname[64];
   for (int c = 0; c < nchunk; ++c) {
@@ -473,10 +478,11 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog) {
   return k;
 }
 
-cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads, size_t smem,
-                       int grid, cudaStream_t stream) {
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads,
+                       size_t smem_double, int sms, cudaStream_t stream) {
   void* args[] = {(void*)&d_prog, (void*)&psi};
-  CUresult r = driver().launch((CUfunction)k.functions[p], grid, 1, 1, threads, 1, 1, (unsigned)smem,
+  const unsigned smem = (unsigned)(k.blocks == 1 ? smem_double : smem_double / 2);
+  CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)(k.blocks * sms), 1, 1, threads, 1, 1, smem,
                                (CUstream)stream, args, nullptr);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
 }

@@ -15,10 +15,18 @@
 
 namespace qsb {
 
+// Geometry of the specialised kernels.  The register bits per thread (lr) are fixed when
+// the program is planned (2^(m - lr) threads per block); blocks = 1 double-buffers the
+// group loads inside a block, blocks = 2 gives each of two resident blocks one buffer.
+struct JitConfig {
+  int blocks = 1;
+};
+
 struct JitKernels {
   std::vector<void*> functions;  // CUfunction per pass
   std::vector<void*> modules;    // CUmodule per compiled chunk
   uint64_t key = 0;
+  int blocks = 1;
   double compile_seconds = 0.0;
   ~JitKernels();
 };
@@ -26,18 +34,19 @@ struct JitKernels {
 // True when NVRTC and the driver entry points are available (message otherwise).
 bool jit_available(std::string* why);
 
-// Cache key of a complex64 program (structure + entry classes).
-uint64_t jit_key(const Program& prog);
+// Cache key of a complex64 program (structure + entry classes + geometry).
+uint64_t jit_key(const Program& prog, const JitConfig& cfg);
 
 // CUDA source of the specialised kernels for passes [pass_begin, pass_end).
-std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key);
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg);
 
 // Compile (cached) the kernels of every pass of a complex64 program.
-std::shared_ptr<JitKernels> jit_get(const Program& prog);
+std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
 
 // Launch the specialised kernel of pass p (one launch per pass, no grid barrier).
-cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads, size_t smem,
-                       int grid, cudaStream_t stream);
+// smem_double = bytes of two group buffers (Program::max_smem).
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads,
+                       size_t smem_double, int sms, cudaStream_t stream);
 
 // Compile a program's source on the host only (tests; returns the NVRTC log on failure).
 bool jit_compile_check(const Program& prog, std::string* log);

@@ -126,7 +126,9 @@ __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const 
 
 // Exec::run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
 // thread's registers a[] (pb = physical index of the thread's register-0 amplitude).
-template <typename Real, int LR, typename Exec>
+// kDouble: two group buffers per block (the next group's copies overlap this group's
+// phases); otherwise one buffer and two resident blocks per SM overlap each other.
+template <typename Real, int LR, typename Exec, bool kDouble = true>
 __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi,
                                           int pass_begin, int pass_end, unsigned* bar, unsigned* err,
                                           uint64_t barrier_limit_ns) {
@@ -166,17 +168,25 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
     __syncthreads();
     const uint64_t ngroups = 1ull << pd.ngbits;
     const bool active = (int)t < T;
-    C* bufs[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + (1u << m)};
+    C* bufs[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + (kDouble ? (1u << m) : 0u)};
 
     uint64_t g = blockIdx.x;
-    if (g < ngroups) prefetch_group<Real>(bufs[0], psi, g, pd, pv, T, V);
-    cp_async_commit();
+    if (kDouble) {
+      if (g < ngroups) prefetch_group<Real>(bufs[0], psi, g, pd, pv, T, V);
+      cp_async_commit();
+    }
     for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
       C* sm = bufs[it & 1];
-      const uint64_t gn = g + gridDim.x;
-      if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gn, pd, pv, T, V);
-      cp_async_commit();
-      cp_async_wait<1>();
+      if (kDouble) {
+        const uint64_t gn = g + gridDim.x;
+        if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gn, pd, pv, T, V);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        prefetch_group<Real>(sm, psi, g, pd, pv, T, V);
+        cp_async_commit();
+        cp_async_wait<0>();
+      }
       __syncthreads();
       // ---- phases ----
       for (int h = 0; h < pd.nphase; ++h) {

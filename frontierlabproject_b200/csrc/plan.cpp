@@ -99,6 +99,86 @@ COp classify(const QOp& op) {
 }
 
 // ---------------------------------------------------------------------------------
+// Global-phase normalisation: U = e^{i a} V with V of a cheaper class (SX = e^{i pi/4} RX(pi/2),
+// RZ(t) = e^{-i t/2} diag(1, e^{i t}), diagonal 2q gates with d0 = 1).  The product of the
+// extracted phases is multiplied back into one later gate that carries coefficients, so the
+// state (global phase included) is unchanged up to rounding.
+// ---------------------------------------------------------------------------------
+namespace {
+
+cplx snap(cplx z, double scale) {
+  const double eps = 1e-14 * scale;
+  return cplx(std::abs(z.real()) < eps ? 0.0 : z.real(), std::abs(z.imag()) < eps ? 0.0 : z.imag());
+}
+
+int cost_1q(const cplx* U) {
+  if (is_zero(U[1]) && is_zero(U[2])) return is_one(U[0]) ? 1 : 2;
+  bool real = true, reim = true;
+  for (int i = 0; i < 4; ++i) if (U[i].imag() != 0.0) real = false;
+  if (U[0].imag() != 0.0 || U[3].imag() != 0.0 || U[1].real() != 0.0 || U[2].real() != 0.0) reim = false;
+  return (real || reim) ? 3 : 4;
+}
+
+}  // namespace
+
+void normalize_global_phase(std::vector<QOp>& ops) {
+  cplx total(1.0, 0.0);
+  int absorber = -1;
+  for (size_t i = 0; i < ops.size(); ++i) {
+    QOp& o = ops[i];
+    const int d = o.arity == 1 ? 2 : 4;
+    double scale = 0.0;
+    for (int e = 0; e < d * d; ++e) scale = std::max(scale, std::abs(o.U[e]));
+    if (scale == 0.0) continue;
+    if (o.arity == 1) {
+      const bool diag = is_zero(o.U[1]) && is_zero(o.U[2]);
+      int best = cost_1q(o.U);
+      cplx best_ph(1.0, 0.0), bestV[4];
+      for (int e = 0; e < 4; ++e) {
+        if (std::abs(o.U[e]) < 1e-12 * scale) continue;
+        const cplx ph = o.U[e] / std::abs(o.U[e]);
+        cplx V[4];
+        for (int k = 0; k < 4; ++k) V[k] = snap(o.U[k] / ph, scale);
+        // a unit-modulus diagonal entry divided by its own phase is exactly one
+        if (diag && e == 0 && std::abs(std::abs(o.U[0]) - 1.0) < 1e-14) V[0] = cplx(1.0, 0.0);
+        const int c = cost_1q(V);
+        if (c < best) {
+          best = c;
+          best_ph = ph;
+          for (int k = 0; k < 4; ++k) bestV[k] = V[k];
+        }
+      }
+      if (best_ph != cplx(1.0, 0.0)) {
+        for (int k = 0; k < 4; ++k) o.U[k] = bestV[k];
+        total *= best_ph;
+      }
+      if (!(is_zero(o.U[0]) && is_zero(o.U[3]) && is_one(o.U[1]) && is_one(o.U[2]))) absorber = (int)i;
+    } else {
+      bool diag = true;
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+          if (r != c && !is_zero(o.U[4 * r + c])) diag = false;
+      if (diag && !is_one(o.U[0]) && std::abs(std::abs(o.U[0]) - 1.0) < 1e-14) {
+        const cplx ph = o.U[0] / std::abs(o.U[0]);
+        for (int k = 0; k < 4; ++k) o.U[5 * k] = snap(o.U[5 * k] / ph, scale);
+        o.U[0] = cplx(1.0, 0.0);
+        total *= ph;
+      }
+    }
+  }
+  if (total == cplx(1.0, 0.0)) return;
+  if (absorber >= 0) {
+    for (int k = 0; k < 4; ++k) ops[absorber].U[k] *= total;
+  } else {
+    QOp g;
+    g.arity = 1;
+    g.q0 = 0;
+    g.U[0] = total; g.U[1] = 0.0; g.U[2] = 0.0; g.U[3] = total;
+    ops.push_back(g);
+  }
+}
+
+// ---------------------------------------------------------------------------------
 // Greedy + hill-climbing choice of a bit set of size `cap` (containing `forced`) that
 // executes the longest dependency-closed run of the remaining ops.
 // ---------------------------------------------------------------------------------
@@ -362,7 +442,7 @@ static std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype)
 }
 
 Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops, int n,
-                       int dtype) {
+                       int dtype, int r_req) {
   Program prog;
   std::vector<PassDesc> pd;
   std::vector<PhaseDesc> phd;
@@ -377,8 +457,8 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
     d.m = (int)ps.sbits.size();
     // register bits per thread are fixed by the dtype (the kernel's template parameter);
     // 2^(r - item bits) = 16 load/store items per thread
-    const int r = dtype == 0 ? 5 : 4;
-    if (d.m < r || d.m - r > 8) throw std::runtime_error("encoder: pass size outside the kernel's geometry");
+    const int r = r_req > 0 ? r_req : (dtype == 0 ? 5 : 4);
+    if (d.m < r || d.m - r > 9) throw std::runtime_error("encoder: pass size outside the kernel's geometry");
     d.r = r;
     d.phase0 = (int)phd.size();
     d.nphase = (int)ps.phases.size();

@@ -32,6 +32,10 @@ struct COp {
 
 COp classify(const QOp& op);
 
+// Rewrites 1q gates and diagonal 2q gates as e^{ia} V with V of a cheaper class and folds
+// the product of the phases into one later 1q gate (or appends a global-phase gate).
+void normalize_global_phase(std::vector<QOp>& ops);
+
 struct PlanConfig {
   int m = 13;             // local bits per pass
   int r = 5;              // register bits per thread
@@ -68,8 +72,10 @@ struct Program {
   bool has_gates = false;  // at least one gate instruction
 };
 
+// r_req: register bits per thread (the generic kernel's fixed value when <= 0:
+// 5 for complex64, 4 for complex128; specialised kernels may use others).
 Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops,
-                       int n, int dtype);
+                       int n, int dtype, int r_req = 0);
 
 // Reference interpretation of a program on host memory (used by CPU tests of the planner).
 void emulate_program(const uint8_t* prog, void* state, int n, int dtype);

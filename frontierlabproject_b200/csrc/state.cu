@@ -77,6 +77,8 @@ struct qs_state {
   PlanConfig cfg;
   int grid_mult = 0;
   int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
+  int jit_lr = 4;          // register bits per thread of the specialised kernels
+  int jit_blocks = 1;      // resident blocks per SM of the specialised kernels
   // device scratch: program buffer, control words (barrier x2, error), accumulators
   uint8_t* d_prog = nullptr;
   size_t prog_cap = 0;
@@ -152,10 +154,20 @@ struct qs_state {
     return per_sm * device_sm_count();
   }
 
-  void run_program(const Program& prog, int mode) {
+  // whether the next graphed flush of gates uses the specialised kernels
+  bool want_jit() const {
+    if (dtype != 0 || queue_mode != QS_MODE_GRAPHED) return false;
+    if (jit_mode < 0 || (jit_mode == 0 && n < 20)) return false;
+    std::string why;
+    if (jit_available(&why)) return true;
+    if (jit_mode > 0) throw InvalidArg{"jit requested but unavailable: " + why};
+    return false;
+  }
+
+  void run_program(const Program& prog, int mode, bool use_jit = false) {
     if (prog.npass == 0) return;
     upload(prog);
-    int grid = grid_for_program(prog);
+    const int grid = use_jit ? 0 : grid_for_program(prog);
     if (mode == QS_MODE_COOPERATIVE) {
       CK(cudaMemsetAsync(d_ctl, 0, 2 * sizeof(unsigned), stream));
       CK(launch_pass_kernel(dtype, d_prog, psi, 0, prog.npass, prog.threads, prog.max_smem, grid, true, d_ctl,
@@ -164,10 +176,12 @@ struct qs_state {
     } else {
       // specialised kernels for large complex64 states (compiled once per structure)
       std::shared_ptr<JitKernels> jk;
-      if (dtype == 0 && prog.has_gates && (jit_mode > 0 || (jit_mode == 0 && n >= 20))) {
-        std::string why;
-        if (jit_available(&why)) jk = jit_get(prog);
-        else if (jit_mode > 0) throw InvalidArg{"jit requested but unavailable: " + why};
+      if (use_jit) {
+        JitConfig jc;
+        jc.blocks = jit_blocks;
+        jk = jit_get(prog, jc);
+        st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
+        jk->compile_seconds = 0.0;  // counted once
       }
       const uint64_t skey = jk ? jk->key : prog.structure_hash;
       const uint64_t key = skey ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
@@ -179,7 +193,7 @@ struct qs_state {
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int p = 0; p < prog.npass && e == cudaSuccess; ++p)
-          e = jk ? jit_launch(*jk, p, d_prog, psi, prog.threads, prog.max_smem, grid, stream)
+          e = jk ? jit_launch(*jk, p, d_prog, psi, prog.threads, prog.max_smem, device_sm_count(), stream)
                  : launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false,
                                       d_ctl, d_ctl + 2, kBarrierLimitNs, stream);
         cudaError_t e2 = cudaStreamEndCapture(stream, &g);
@@ -228,13 +242,20 @@ struct qs_state {
     }
     std::vector<COp> cops;
     cops.reserve(ops.size());
+    normalize_global_phase(ops);
     for (const QOp& o : ops) cops.push_back(classify(o));
+    const bool use_jit = want_jit();
     PlanConfig c = eff_cfg();
+    if (use_jit) {
+      c.r = jit_lr;
+      c.m = std::max(c.r, std::min(cfg.m, n));
+    }
     // The plan depends on the gate classes and bits only, not on the matrix values:
     // repeated circuits (parameter sweeps, benchmark steps) reuse it.
     uint64_t key = 1469598103934665603ull;
     auto mix = [&key](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
     mix((uint64_t)n); mix((uint64_t)dtype); mix((uint64_t)c.m); mix((uint64_t)c.k); mix((uint64_t)c.hill_iters);
+    mix((uint64_t)c.r);
     for (const COp& o : cops) mix(((uint64_t)o.kind << 16) | ((uint64_t)(o.a & 0xff) << 8) | (uint64_t)(o.b & 0xff));
     const std::vector<PlannedPass>* passes = nullptr;
     for (auto& e : plan_cache)
@@ -245,8 +266,8 @@ struct qs_state {
       passes = &plan_cache.back().second.second;
       st.plans += 1;
     }
-    Program prog = encode_program(*passes, cops, n, dtype);
-    run_program(prog, queue_mode);
+    Program prog = encode_program(*passes, cops, n, dtype, c.r);
+    run_program(prog, queue_mode, use_jit);
   }
 
   // move data so that physical bit p holds layout position p
@@ -588,12 +609,16 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     if (c->m < reg_bits(s->dtype) + 1 || c->m > mmax) throw InvalidArg{"config: m out of range"};
     if (c->k < 1 || c->k > c->m) throw InvalidArg{"config: k out of range"};
     if (c->hill_iters < 0) throw InvalidArg{"config: hill_iters must be >= 0"};
+    if (c->jit_lr < 3 || c->jit_lr > 5 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
+    if (c->jit_blocks < 1 || c->jit_blocks > 2) throw InvalidArg{"config: jit_blocks must be 1 or 2"};
     s->flush();
     s->cfg.m = c->m;
     s->cfg.k = c->k;
     s->cfg.hill_iters = c->hill_iters;
     s->grid_mult = c->grid_mult;
     s->jit_mode = c->jit;
+    s->jit_lr = c->jit_lr;
+    s->jit_blocks = c->jit_blocks;
   });
 }
 
@@ -602,6 +627,8 @@ int qs_get_config(qs_state* s, qs_config* c) {
     if (!s || !c) throw InvalidArg{"null argument"};
     c->m = s->cfg.m; c->k = s->cfg.k; c->hill_iters = s->cfg.hill_iters; c->grid_mult = s->grid_mult;
     c->jit = s->jit_mode;
+    c->jit_lr = s->jit_lr;
+    c->jit_blocks = s->jit_blocks;
   });
 }
 
@@ -702,6 +729,7 @@ int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs
     if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
+    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
     auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
     int ph = 0;
@@ -716,6 +744,7 @@ int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const
     if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 24) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
+    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
     auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
     Program prog = encode_program(passes, c, num_qubits, dtype);
@@ -723,16 +752,26 @@ int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const
   });
 }
 
-int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps) {
+int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps, char* logbuf,
+                 int logcap) {
   return guard([&] {
     if (num_qubits < reg_bits(0) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, 0, false);
     std::vector<COp> c;
+    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
-    auto passes = plan_passes(c, num_qubits, cfg_from(0, num_qubits, cfg));
-    Program prog = encode_program(passes, c, num_qubits, 0);
+    PlanConfig pc = cfg_from(0, num_qubits, cfg);
+    pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) ? cfg->jit_lr : 4;
+    auto passes = plan_passes(c, num_qubits, pc);
+    Program prog = encode_program(passes, c, num_qubits, 0, pc.r);
     std::string log;
-    if (!jit_compile_check(prog, &log)) throw InvalidArg{"jit compile failed:\n" + log.substr(0, 4000)};
+    const bool ok = jit_compile_check(prog, &log);
+    if (logbuf && logcap > 0) {
+      const size_t k = std::min<size_t>(log.size(), (size_t)logcap - 1);
+      std::memcpy(logbuf, log.data(), k);
+      logbuf[k] = '\0';
+    }
+    if (!ok) throw InvalidArg{"jit compile failed:\n" + log.substr(0, 4000)};
     if (sweeps) *sweeps = prog.npass;
   });
 }

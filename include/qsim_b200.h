@@ -62,6 +62,8 @@ typedef struct {
   int grid_mult;  /* resident blocks per SM used by the pass kernel (0 = occupancy) */
   int jit;        /* plan-time specialised kernels in graphed mode: 0 auto (complex64,
                      >= 20 qubits), 1 always (complex64), -1 never */
+  int jit_lr;     /* register bits per thread of the specialised kernels (3..5) */
+  int jit_blocks; /* resident blocks per SM of the specialised kernels (1 or 2) */
 } qs_config;
 
 typedef struct {
@@ -75,6 +77,7 @@ typedef struct {
   unsigned long long flushes;        /* planned executions */
   unsigned long long permutes;       /* permute() calls */
   unsigned long long plans;          /* pass plans computed (cache misses) */
+  unsigned long long jit_compile_ms; /* host time spent compiling specialised kernels */
 } qs_stats;
 
 /* Library */
@@ -151,8 +154,10 @@ QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, c
  * applies ops to the host state psi (2^n entries, dtype precision). */
 QS_API int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg, void* psi);
 /* Generate and compile (NVRTC, sm_100a, host only) the specialised kernels of the planned
- * program for ops; returns QS_ERR_INVALID with the compiler log on failure. */
-QS_API int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps);
+ * complex64 program for ops; returns QS_ERR_INVALID with the compiler log on failure.
+ * log (optional, logcap bytes) receives the compiler log (ptxas resource usage). */
+QS_API int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cfg, int* sweeps, char* log,
+                        int logcap);
 /* Host emulation of the in-place permutation program: perm[b] = destination bit. */
 QS_API int qs_perm_emulate(int num_qubits, int dtype, const int* perm, const qs_config* cfg, void* psi,
                     int* sweeps);

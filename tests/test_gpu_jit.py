@@ -18,11 +18,19 @@ def test_jit_source_compiles_for_sm100a(native_lib):
     qc = _mixed(12, 3)
     b = _OpBatch(ops_of(qc), 0)
     sw = ctypes.c_int()
-    rc = native_lib.qs_jit_check(12, b.ptr, len(b), None, ctypes.byref(sw))
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = native_lib.qs_jit_check(12, b.ptr, len(b), None, ctypes.byref(sw), log, len(log))
     if rc != 0 and b"NVRTC" in native_lib.qs_last_error() and b"not found" in native_lib.qs_last_error():
         pytest.skip("NVRTC unavailable")
     assert rc == 0, native_lib.qs_last_error().decode()
     assert sw.value >= 1
+    # specialised kernels hold all amplitudes in registers: no local-memory spills
+    text = log.value.decode()
+    assert "registers" in text
+    assert "0 bytes spill stores" in text and "bytes spill stores" in text
+    for line in text.splitlines():
+        if "spill stores" in line:
+            assert line.strip().startswith("0 bytes stack frame") or " 0 bytes spill stores" in line, line
 
 
 def _run_jit(qc, nl, **kw):
