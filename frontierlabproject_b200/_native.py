@@ -70,6 +70,8 @@ _SIGS = {
     "qs_get_pos2bit": [c_void_p, c_void_p, c_int],
     "qs_norm_squared": [c_void_p, POINTER(c_double)],
     "qs_inner_product": [c_void_p, c_void_p, POINTER(c_double), POINTER(c_double)],
+    "qs_expect_zz_x": [c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_double)],
+    "qs_adjoint_sweep": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int],
     "qs_apply_1q_gate": [c_void_p, c_int, c_void_p, c_int, c_int, c_void_p],
     "qs_apply_2q_gate": [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p],
     "qs_permute_scatter": [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p],

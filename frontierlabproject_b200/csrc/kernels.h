@@ -26,6 +26,14 @@ cudaError_t launch_norm2(int dtype, const void* psi, int n, double* acc, cudaStr
 cudaError_t launch_inner(int dtype, const void* a, const void* b, int n, double* acc2, cudaStream_t s);
 cudaError_t launch_set_basis(int dtype, void* psi, int n, uint64_t index, cudaStream_t s);
 
+// adjoint differentiation (kern_adjoint.cu)
+cudaError_t launch_zz_x(int dtype, const void* psi, void* lam, int n, const double* a, const double* b,
+                        double* energy, cudaStream_t s);
+cudaError_t launch_adjoint_gate1(int dtype, void* psi, void* lam, int n, int q, const std::complex<double>* Ud,
+                                 int gen, double* acc, cudaStream_t s);
+cudaError_t launch_adjoint_gate2(int dtype, void* psi, void* lam, int n, int q0, int q1,
+                                 const std::complex<double>* Ud, cudaStream_t s);
+
 int device_sm_count();
 
 }  // namespace qsb

@@ -675,6 +675,75 @@ int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im) {
   });
 }
 
+int qs_expect_zz_x(qs_state* psi, qs_state* lam, const double* a, const double* b, double* energy) {
+  return guard([&] {
+    if (!psi || !lam || !a || !b || !energy) throw InvalidArg{"null argument"};
+    if (psi->n != lam->n || psi->dtype != lam->dtype) throw InvalidArg{"states differ in size or dtype"};
+    if (psi == lam) throw InvalidArg{"psi and lam must be different states"};
+    psi->materialize();
+    lam->flush();
+    CK(cudaStreamSynchronize(lam->stream));
+    lam->queue.clear();
+    for (int p = 0; p < lam->n; ++p) lam->pos2bit[p] = p;
+    CK(cudaMemsetAsync(psi->d_acc, 0, sizeof(double), psi->stream));
+    CK(launch_zz_x(psi->dtype, psi->psi, lam->psi, psi->n, a, b, psi->d_acc, psi->stream));
+    CK(cudaMemcpyAsync(psi->h_acc, psi->d_acc, sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
+    CK(cudaStreamSynchronize(psi->stream));
+    *energy = psi->h_acc[0];
+    psi->st.launches += 1;
+  });
+}
+
+int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nops, double* grads, int ngrads) {
+  return guard([&] {
+    if (!psi || !lam || (nops > 0 && !ops) || (ngrads > 0 && !grads)) throw InvalidArg{"null argument"};
+    if (psi->n != lam->n || psi->dtype != lam->dtype) throw InvalidArg{"states differ in size or dtype"};
+    if (psi == lam) throw InvalidArg{"psi and lam must be different states"};
+    const int n = psi->n;
+    for (int i = 0; i < nops; ++i) {
+      const qs_adj_op& o = ops[i];
+      if (!o.U) throw InvalidArg{"adjoint: null gate matrix"};
+      if (o.kind == QS_OP_1Q) {
+        if (o.q0 < 0 || o.q0 >= n) throw InvalidArg{"adjoint: invalid q0"};
+        if (o.gen < 0 || o.gen > 3) throw InvalidArg{"adjoint: generator must be 0..3"};
+        if (o.gen && (o.grad_index < 0 || o.grad_index >= ngrads)) throw InvalidArg{"adjoint: grad_index out of range"};
+      } else if (o.kind == QS_OP_2Q) {
+        if (o.q0 < 0 || o.q0 >= n || o.q1 < 0 || o.q1 >= n || o.q0 == o.q1)
+          throw InvalidArg{"adjoint: invalid q0/q1"};
+        if (o.gen != 0) throw InvalidArg{"adjoint: two-qubit gates carry no parameter"};
+      } else {
+        throw InvalidArg{"adjoint: unknown op kind: " + std::to_string(o.kind)};
+      }
+    }
+    psi->materialize();
+    lam->materialize();
+    CK(cudaStreamSynchronize(lam->stream));
+    double* d_grad = nullptr;
+    CK(cudaMallocAsync(&d_grad, std::max(1, ngrads) * sizeof(double), psi->stream));
+    CK(cudaMemsetAsync(d_grad, 0, std::max(1, ngrads) * sizeof(double), psi->stream));
+    for (int i = nops - 1; i >= 0; --i) {
+      const qs_adj_op& o = ops[i];
+      if (o.kind == QS_OP_1Q) {
+        cplx Ud[4];
+        for (int r = 0; r < 2; ++r)
+          for (int c = 0; c < 2; ++c) Ud[2 * r + c] = std::conj(cplx(o.U[2 * (2 * c + r)], o.U[2 * (2 * c + r) + 1]));
+        CK(launch_adjoint_gate1(psi->dtype, psi->psi, lam->psi, n, o.q0, Ud, o.gen,
+                                o.gen ? d_grad + o.grad_index : d_grad, psi->stream));
+      } else {
+        cplx Ud[16];
+        for (int r = 0; r < 4; ++r)
+          for (int c = 0; c < 4; ++c) Ud[4 * r + c] = std::conj(cplx(o.U[2 * (4 * c + r)], o.U[2 * (4 * c + r) + 1]));
+        CK(launch_adjoint_gate2(psi->dtype, psi->psi, lam->psi, n, o.q0, o.q1, Ud, psi->stream));
+      }
+      psi->st.launches += 1;
+      psi->st.gate_sweeps += 2;
+    }
+    if (ngrads > 0) CK(cudaMemcpyAsync(grads, d_grad, ngrads * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
+    CK(cudaFreeAsync(d_grad, psi->stream));
+    CK(cudaStreamSynchronize(psi->stream));
+  });
+}
+
 int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream) {
   return guard([&] {
     if (!psi || !U) throw InvalidArg{"null argument"};

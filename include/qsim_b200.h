@@ -137,6 +137,31 @@ QS_API int qs_get_pos2bit(qs_state* s, int* out, int n);
 QS_API int qs_norm_squared(qs_state* s, double* out);
 QS_API int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im);
 
+/* Adjoint differentiation (no counterpart in the reference executor).
+ * qs_expect_zz_x: lam <- H psi and energy = <psi|H|psi> (FP64) for
+ * H = sum_i a_i Z_i Z_{(i+1) mod n} + b_i X_i; psi and lam are states of equal size/dtype. */
+QS_API int qs_expect_zz_x(qs_state* psi, qs_state* lam, const double* a, const double* b, double* energy);
+
+/* One gate of a circuit for the reverse sweep.  U: host complex128 matrix (4 or 16
+ * entries, row-major, index b_q0 + 2*b_q1) of the forward gate; gen: generator of a
+ * parameterised rotation R(theta) = exp(-i theta G / 2): 0 none, 1 X, 2 Y, 3 Z. */
+typedef struct {
+  int kind; /* QS_OP_1Q or QS_OP_2Q */
+  int q0;
+  int q1;
+  int gen;
+  int grad_index; /* slot of dE/dtheta in grads (ignored when gen == 0) */
+  int pad;
+  const double* U;
+} qs_adj_op;
+
+/* Reverse sweep: psi holds U|0>, lam holds H psi (qs_expect_zz_x).  For k = nops-1 .. 0:
+ * grads[grad_index] += Im <lam|G|psi> (FP64), then psi <- U_k^dagger psi, lam <- U_k^dagger lam.
+ * Ops use layout positions of the states (identity layout after qs_expect_zz_x).
+ * grads (host, ngrads doubles) is overwritten. */
+QS_API int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nops, double* grads,
+                            int ngrads);
+
 /* Module-level apply_1q_gate / apply_2q_gate (bindings.cpp:931-1001): gate on a raw
  * device array psi of 2^num_qubits amplitudes; U is a host matrix; stream may be NULL. */
 QS_API int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream);
