@@ -287,7 +287,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", type=int, default=0, help="0 auto, 1 always, -1 never")
-    ap.add_argument("--jit-lr", type=int, default=4)
+    ap.add_argument("--jit-lr", type=int, default=5)
     ap.add_argument("--jit-blocks", type=int, default=1)
     ap.add_argument("--m", type=int, default=13)
     ap.add_argument("--no-adjoint", action="store_true")

@@ -364,8 +364,9 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       G.o << "}break;\n";
     }
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
-    // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block
-    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(" << (1 << (pd.m - pd.r)) << ","
+    // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block.  The bound
+    // is the block size every pass of the program is launched with (>= this pass's threads).
+    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ","
         << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi)"
         << "{qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
         << ">(prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
@@ -484,7 +485,10 @@ cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* 
   const unsigned smem = (unsigned)(k.blocks == 1 ? smem_double : smem_double / 2);
   CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)(k.blocks * sms), 1, 1, threads, 1, 1, smem,
                                (CUstream)stream, args, nullptr);
-  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+  if (r == CUDA_SUCCESS) return cudaSuccess;
+  // launch-time rejections (configuration) are reported as such, not as a kernel failure
+  if (r == CUDA_ERROR_INVALID_VALUE || r == CUDA_ERROR_LAUNCH_OUT_OF_RESOURCES) return cudaErrorInvalidConfiguration;
+  return cudaErrorLaunchFailure;
 }
 
 }  // namespace qsb

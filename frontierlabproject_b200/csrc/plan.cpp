@@ -99,10 +99,7 @@ COp classify(const QOp& op) {
 }
 
 // ---------------------------------------------------------------------------------
-// Global-phase normalisation: U = e^{i a} V with V of a cheaper class (SX = e^{i pi/4} RX(pi/2),
-// RZ(t) = e^{-i t/2} diag(1, e^{i t}), diagonal 2q gates with d0 = 1).  The product of the
-// extracted phases is multiplied back into one later gate that carries coefficients, so the
-// state (global phase included) is unchanged up to rounding.
+// helpers of the per-pass scalar extraction
 // ---------------------------------------------------------------------------------
 namespace {
 
@@ -111,71 +108,100 @@ cplx snap(cplx z, double scale) {
   return cplx(std::abs(z.real()) < eps ? 0.0 : z.real(), std::abs(z.imag()) < eps ? 0.0 : z.imag());
 }
 
-int cost_1q(const cplx* U) {
-  if (is_zero(U[1]) && is_zero(U[2])) return is_one(U[0]) ? 1 : 2;
-  bool real = true, reim = true;
-  for (int i = 0; i < 4; ++i) if (U[i].imag() != 0.0) real = false;
-  if (U[0].imag() != 0.0 || U[3].imag() != 0.0 || U[1].real() != 0.0 || U[2].real() != 0.0) reim = false;
-  return (real || reim) ? 3 : 4;
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// Per-pass scalar extraction: each gate with coefficients is written s * V with one entry
+// of V exactly 1, choosing the entry that leaves the most entries in {0, +-1, +-i} (an
+// add instead of a multiply in the specialised kernels): H = (1/sqrt2)[[1,1],[1,-1]],
+// RX(t) = cos(t/2)[[1,-i tan],[-i tan,1]], SX = ((1+i)/2)[[1,-i],[-i,1]], RZ = e^{-it/2}
+// diag(1, e^{it}).  The product of a pass's scalars is multiplied into one gate of the
+// same pass, so magnitudes stay bounded in single precision and the state is unchanged.
+// ---------------------------------------------------------------------------------
+namespace {
+
+int entry_cost(const cplx& z) {
+  const double r = z.real(), i = z.imag();
+  if (r == 0.0 && i == 0.0) return 0;
+  if ((i == 0.0 && (r == 1.0 || r == -1.0)) || (r == 0.0 && (i == 1.0 || i == -1.0))) return 1;
+  if (i == 0.0 || r == 0.0) return 2;
+  return 4;
+}
+
+int matrix_cost(const cplx* U, int d) {
+  int c = 0;
+  for (int e = 0; e < d * d; ++e) c += entry_cost(U[e]);
+  return c;
+}
+
+bool carries_coefficients(const QOp& o) {
+  // permutations (X, CX, SWAP) carry none; everything else is multiplied entry by entry
+  const int d = o.arity == 1 ? 2 : 4;
+  for (int e = 0; e < d * d; ++e) {
+    const cplx z = o.U[e];
+    if (!(z == cplx(0, 0) || z == cplx(1, 0))) return true;
+  }
+  return false;
+}
+
+// the rewritten gate keeps the shape the planner used: same staged/register needs, same
+// operand roles, same diagonal / controlled / dense family
+bool same_shape(const QOp& o, const cplx* V) {
+  QOp b = o;
+  const int d = o.arity == 1 ? 2 : 4;
+  for (int k = 0; k < d * d; ++k) b.U[k] = V[k];
+  const COp x = classify(o), y = classify(b);
+  if (x.need != y.need || x.touch != y.touch || x.a != y.a || x.b != y.b) return false;
+  if (o.arity == 2) return x.kind == y.kind;
+  return (x.kind == GK_1Q_DIAG) == (y.kind == GK_1Q_DIAG) && (x.kind == GK_1Q_X) == (y.kind == GK_1Q_X);
 }
 
 }  // namespace
 
-void normalize_global_phase(std::vector<QOp>& ops) {
+void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops) {
   cplx total(1.0, 0.0);
-  int absorber = -1;
-  for (size_t i = 0; i < ops.size(); ++i) {
-    QOp& o = ops[i];
+  int absorber = -1, absorber_cost = -1;
+  for (int oi : pass_ops) {
+    QOp& o = ops[oi];
     const int d = o.arity == 1 ? 2 : 4;
+    if (!carries_coefficients(o)) continue;
     double scale = 0.0;
     for (int e = 0; e < d * d; ++e) scale = std::max(scale, std::abs(o.U[e]));
     if (scale == 0.0) continue;
-    if (o.arity == 1) {
-      const bool diag = is_zero(o.U[1]) && is_zero(o.U[2]);
-      int best = cost_1q(o.U);
-      cplx best_ph(1.0, 0.0), bestV[4];
-      for (int e = 0; e < 4; ++e) {
-        if (std::abs(o.U[e]) < 1e-12 * scale) continue;
-        const cplx ph = o.U[e] / std::abs(o.U[e]);
-        cplx V[4];
-        for (int k = 0; k < 4; ++k) V[k] = snap(o.U[k] / ph, scale);
-        // a unit-modulus diagonal entry divided by its own phase is exactly one
-        if (diag && e == 0 && std::abs(std::abs(o.U[0]) - 1.0) < 1e-14) V[0] = cplx(1.0, 0.0);
-        const int c = cost_1q(V);
-        if (c < best) {
-          best = c;
-          best_ph = ph;
-          for (int k = 0; k < 4; ++k) bestV[k] = V[k];
-        }
-      }
-      if (best_ph != cplx(1.0, 0.0)) {
-        for (int k = 0; k < 4; ++k) o.U[k] = bestV[k];
-        total *= best_ph;
-      }
-      if (!(is_zero(o.U[0]) && is_zero(o.U[3]) && is_one(o.U[1]) && is_one(o.U[2]))) absorber = (int)i;
-    } else {
-      bool diag = true;
-      for (int r = 0; r < 4; ++r)
-        for (int c = 0; c < 4; ++c)
-          if (r != c && !is_zero(o.U[4 * r + c])) diag = false;
-      if (diag && !is_one(o.U[0]) && std::abs(std::abs(o.U[0]) - 1.0) < 1e-14) {
-        const cplx ph = o.U[0] / std::abs(o.U[0]);
-        for (int k = 0; k < 4; ++k) o.U[5 * k] = snap(o.U[5 * k] / ph, scale);
-        o.U[0] = cplx(1.0, 0.0);
-        total *= ph;
+    int best = matrix_cost(o.U, d);
+    int best_e = -1;
+    cplx bestV[16];
+    for (int e = 0; e < d * d; ++e) {
+      if (std::abs(o.U[e]) < 1e-6 * scale) continue;  // keep scaled entries bounded
+      cplx V[16];
+      for (int k = 0; k < d * d; ++k) V[k] = snap(o.U[k] / o.U[e], scale / std::abs(o.U[e]));
+      for (int k = 0; k < d * d; ++k)  // entries equal to the pivot divide to exactly one
+        if (o.U[k] == o.U[e]) V[k] = cplx(1.0, 0.0);
+      V[e] = cplx(1.0, 0.0);
+      const int c = matrix_cost(V, d);
+      if (c < best && same_shape(o, V)) {
+        best = c;
+        best_e = e;
+        for (int k = 0; k < d * d; ++k) bestV[k] = V[k];
       }
     }
+    if (best_e >= 0) {
+      total *= o.U[best_e];
+      for (int k = 0; k < d * d; ++k) o.U[k] = bestV[k];
+    }
+    // absorber: a gate whose shape survives scaling, and whose cost grows least
+    const COp c0 = classify(o);
+    const bool can_absorb = o.arity == 1 || c0.kind == GK_2Q_DIAG || c0.kind == GK_2Q_DENSE;
+    if (!can_absorb) continue;
+    int grow = 0;
+    for (int k = 0; k < d * d; ++k) grow += (o.U[k] == cplx(0, 0)) ? 0 : 4 - entry_cost(o.U[k]);
+    if (absorber < 0 || grow < absorber_cost) { absorber = oi; absorber_cost = grow; }
   }
   if (total == cplx(1.0, 0.0)) return;
-  if (absorber >= 0) {
-    for (int k = 0; k < 4; ++k) ops[absorber].U[k] *= total;
-  } else {
-    QOp g;
-    g.arity = 1;
-    g.q0 = 0;
-    g.U[0] = total; g.U[1] = 0.0; g.U[2] = 0.0; g.U[3] = total;
-    ops.push_back(g);
-  }
+  if (absorber < 0) throw std::runtime_error("planner: no gate of the pass can absorb its scalar");
+  QOp& a = ops[absorber];
+  const int d = a.arity == 1 ? 2 : 4;
+  for (int k = 0; k < d * d; ++k) a.U[k] *= total;
 }
 
 // ---------------------------------------------------------------------------------

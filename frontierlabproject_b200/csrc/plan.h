@@ -32,9 +32,10 @@ struct COp {
 
 COp classify(const QOp& op);
 
-// Rewrites 1q gates and diagonal 2q gates as e^{ia} V with V of a cheaper class and folds
-// the product of the phases into one later 1q gate (or appends a global-phase gate).
-void normalize_global_phase(std::vector<QOp>& ops);
+// Rewrites the gates of one planned pass as s * V (one entry of V exactly 1, as many
+// entries as possible in {0, +-1, +-i}) and multiplies the product of the scalars into one
+// gate of the pass.  The classification (need/touch bits) of every gate is unchanged.
+void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops);
 
 struct PlanConfig {
   int m = 13;             // local bits per pass

@@ -55,6 +55,16 @@ constexpr uint64_t kBarrierLimitNs = 20ull * 1000ull * 1000ull * 1000ull;  // 20
 
 int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
 
+// Encode the planned passes after the per-pass scalar extraction (which keeps every gate's
+// planned shape, so the plan made from the original gates stays valid).
+Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& passes, int n, int dtype, int r) {
+  for (const PlannedPass& ps : passes) extract_pass_scalars(ops, ps.ops);
+  std::vector<COp> cops;
+  cops.reserve(ops.size());
+  for (const QOp& o : ops) cops.push_back(classify(o));
+  return encode_program(passes, cops, n, dtype, r);
+}
+
 }  // namespace
 
 struct GraphEntry {
@@ -77,7 +87,7 @@ struct qs_state {
   PlanConfig cfg;
   int grid_mult = 0;
   int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
-  int jit_lr = 4;          // register bits per thread of the specialised kernels
+  int jit_lr = 5;          // register bits per thread of the specialised kernels
   int jit_blocks = 1;      // resident blocks per SM of the specialised kernels
   // device scratch: program buffer, control words (barrier x2, error), accumulators
   uint8_t* d_prog = nullptr;
@@ -242,7 +252,6 @@ struct qs_state {
     }
     std::vector<COp> cops;
     cops.reserve(ops.size());
-    normalize_global_phase(ops);
     for (const QOp& o : ops) cops.push_back(classify(o));
     const bool use_jit = want_jit();
     PlanConfig c = eff_cfg();
@@ -266,7 +275,7 @@ struct qs_state {
       passes = &plan_cache.back().second.second;
       st.plans += 1;
     }
-    Program prog = encode_program(*passes, cops, n, dtype, c.r);
+    Program prog = build_program(ops, *passes, n, dtype, c.r);
     run_program(prog, queue_mode, use_jit);
   }
 
@@ -798,7 +807,6 @@ int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs
     if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
-    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
     auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
     int ph = 0;
@@ -813,10 +821,9 @@ int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const
     if (num_qubits < reg_bits(dtype) + 1 || num_qubits > 24) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
-    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
     auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
-    Program prog = encode_program(passes, c, num_qubits, dtype);
+    Program prog = build_program(q, passes, num_qubits, dtype, 0);
     emulate_program(prog.bytes.data(), psi, num_qubits, dtype);
   });
 }
@@ -827,12 +834,11 @@ int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cf
     if (num_qubits < reg_bits(0) + 1 || num_qubits > 36) throw InvalidArg{"num_qubits out of range"};
     auto q = convert_ops(nullptr, ops, nops, num_qubits, 0, false);
     std::vector<COp> c;
-    normalize_global_phase(q);
     for (auto& o : q) c.push_back(classify(o));
     PlanConfig pc = cfg_from(0, num_qubits, cfg);
-    pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) ? cfg->jit_lr : 4;
+    pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) ? cfg->jit_lr : 5;
     auto passes = plan_passes(c, num_qubits, pc);
-    Program prog = encode_program(passes, c, num_qubits, 0, pc.r);
+    Program prog = build_program(q, passes, num_qubits, 0, pc.r);
     std::string log;
     const bool ok = jit_compile_check(prog, &log);
     if (logbuf && logcap > 0) {
