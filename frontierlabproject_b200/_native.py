@@ -79,6 +79,7 @@ _SIGS = {
     "qs_plan_emulate": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), c_void_p],
     "qs_perm_emulate": [c_int, c_int, c_void_p, POINTER(QsConfig), c_void_p, POINTER(c_int)],
     "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), c_void_p, c_int],
+    "qs_apply_ops_noalloc": [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p],
 }
 
 _lib = None

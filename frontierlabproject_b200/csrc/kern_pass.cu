@@ -13,8 +13,16 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/qsim_b200.h"
 #include "kernels.h"
 #include "pass_body.cuh"
+#include "plan.h"
 #include "qsim.h"
 
 namespace qsb {
@@ -328,4 +336,156 @@ cudaError_t pass_kernel_occupancy(int dtype, int threads, size_t smem, int* bloc
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pass_kernel<double, 4>, threads, smem);
 }
 
+// ------------------------------------------------------------------------------------
+// Allocation-free entry point.  The pass kernel's scratch (the encoded program and the
+// grid-barrier / error words) lives in a fixed device array of this file instead of
+// buffers allocated per state, for callers that cannot allocate device memory.
+// ------------------------------------------------------------------------------------
+constexpr size_t kWorkspaceBytes = size_t(1) << 20;  // 1 MiB: control words + program
+constexpr size_t kWorkspaceCtl = 256;                // barrier (2 words) + error word, padded
+static __device__ __align__(256) unsigned char g_workspace[kWorkspaceBytes];
+
+// variant of the pass kernel whose program and control words sit in g_workspace
+template <typename Real, int LR>
+__global__ void __launch_bounds__(kPassThreads, 1)
+pass_kernel_ws(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi, int pass_begin,
+               int pass_end, unsigned* bar, unsigned* err, uint64_t barrier_limit_ns) {
+  pass_body<Real, LR, InterpExec>(prog, psi, pass_begin, pass_end, bar, err, barrier_limit_ns);
+}
+
+namespace {
+
+// Device address of g_workspace for the current device, looked up once per device (the host
+// symbol g_workspace is not a device address and must never be handed to a kernel).
+cudaError_t workspace_address(unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* addr[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_workspace);
+    if (e != cudaSuccess) return e;
+    addr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = addr[dev];
+  return cudaSuccess;
+}
+
+template <typename Real, int LR>
+cudaError_t launch_ws(const uint8_t* prog, void* psi, int npass, int threads, size_t smem, unsigned* bar,
+                      unsigned* err, uint64_t limit_ns, cudaStream_t stream) {
+  auto kern = pass_kernel_ws<Real, LR>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = per_sm * device_sm_count();
+  using C = typename V2<Real>::T;
+  C* p = reinterpret_cast<C*>(psi);
+  int b = 0;
+  void* args[] = {(void*)&prog, (void*)&p, (void*)&b, (void*)&npass, (void*)&bar, (void*)&err, (void*)&limit_ns};
+  return cudaLaunchCooperativeKernel((void*)kern, dim3(grid), dim3(threads), args, smem, stream);
+}
+
+}  // namespace
+
 }  // namespace qsb
+
+extern "C" QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_op* ops, int nops,
+                                          void* stream) {
+  using namespace qsb;
+  auto fail = [&](const std::string& m) {
+    set_last_error(m);
+    return QS_ERR_INVALID;
+  };
+  auto cuda_fail = [&](cudaError_t e) {
+    fail(std::string("CUDA error: ") + cudaGetErrorString(e));
+    return QS_ERR_CUDA;
+  };
+  if (!psi || (nops > 0 && !ops)) return fail("qs_apply_ops_noalloc: null argument");
+  if (dtype != QS_C64 && dtype != QS_C128) return fail("qs_apply_ops_noalloc: dtype must be QS_C64 or QS_C128");
+  const int r = dtype == 0 ? 5 : 4;
+  if (num_qubits < r + 1 || num_qubits > 36)
+    return fail("qs_apply_ops_noalloc: num_qubits must be in [" + std::to_string(r + 1) + ", 36]");
+  if (nops == 0) return 0;
+  std::vector<QOp> q;
+  try {
+    q.reserve(nops);
+    const size_t esz = dtype == 0 ? 8 : 16;
+    for (int i = 0; i < nops; ++i) {
+      const qs_op& o = ops[i];
+      QOp x;
+      int cnt = 0;
+      if (o.kind == QS_OP_1Q) {
+        if (o.q0 < 0 || o.q0 >= num_qubits) return fail("apply_tile_dev: invalid q0");
+        x.arity = 1; x.q0 = o.q0; cnt = 4;
+      } else if (o.kind == QS_OP_2Q) {
+        if (o.q0 < 0 || o.q0 >= num_qubits || o.q1 < 0 || o.q1 >= num_qubits)
+          return fail("apply_tile_dev: invalid q0/q1");
+        if (o.q0 == o.q1) return fail("apply_tile_dev: q0 == q1");
+        x.arity = 2; x.q0 = o.q0; x.q1 = o.q1; cnt = 16;
+      } else {
+        return fail("apply_tile_dev: unknown op kind: " + std::to_string(o.kind));
+      }
+      if (!o.U) return fail("apply_tile_dev: null gate matrix");
+      if (o.u_on_device) return fail("qs_apply_ops_noalloc: gate matrices must be host memory");
+      for (int k = 0; k < cnt; ++k) {
+        if (esz == 8) {
+          const float* f = static_cast<const float*>(o.U);
+          x.U[k] = cplx(f[2 * k], f[2 * k + 1]);
+        } else {
+          const double* f = static_cast<const double*>(o.U);
+          x.U[k] = cplx(f[2 * k], f[2 * k + 1]);
+        }
+      }
+      q.push_back(x);
+    }
+    std::vector<COp> cops;
+    for (const QOp& o : q) cops.push_back(classify(o));
+    PlanConfig pc;
+    pc.r = r;
+    pc.m = std::max(r, std::min(dtype == 0 ? 13 : 12, num_qubits));
+    auto passes = plan_passes(cops, num_qubits, pc);
+    for (const PlannedPass& ps : passes) extract_pass_scalars(q, ps.ops);
+    cops.clear();
+    for (const QOp& o : q) cops.push_back(classify(o));
+    Program prog = encode_program(passes, cops, num_qubits, dtype, r);
+    if (prog.bytes.size() > kWorkspaceBytes - kWorkspaceCtl)
+      return fail("qs_apply_ops_noalloc: the program of these ops needs " + std::to_string(prog.bytes.size()) +
+                  " bytes; the static workspace holds " + std::to_string(kWorkspaceBytes - kWorkspaceCtl) +
+                  " (split the ops into smaller calls)");
+    unsigned char* ws = nullptr;
+    cudaError_t e = workspace_address(&ws);
+    if (e != cudaSuccess) return cuda_fail(e);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned* ctl = reinterpret_cast<unsigned*>(ws);
+    // the barrier and error words must start at zero for every call
+    if ((e = cudaMemsetAsync(ctl, 0, kWorkspaceCtl, s)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpyAsync(ws + kWorkspaceCtl, prog.bytes.data(), prog.bytes.size(), cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+      return cuda_fail(e);
+    const uint64_t limit = 20ull * 1000 * 1000 * 1000;
+    e = dtype == 0 ? launch_ws<float, 5>(ws + kWorkspaceCtl, psi, prog.npass, prog.threads, prog.max_smem, ctl,
+                                          ctl + 2, limit, s)
+                   : launch_ws<double, 4>(ws + kWorkspaceCtl, psi, prog.npass, prog.threads, prog.max_smem, ctl,
+                                           ctl + 2, limit, s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    unsigned word = 0;
+    if ((e = cudaMemcpyAsync(&word, ctl + 2, sizeof(word), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return cuda_fail(e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e);
+    if (word != 0) {
+      fail("qs_apply_ops_noalloc: device error: a grid barrier wait expired");
+      return QS_ERR_DEVICE;
+    }
+  } catch (const std::exception& ex) {
+    return fail(ex.what());
+  }
+  return 0;
+}

@@ -2,6 +2,7 @@
 #pragma once
 #include <complex>
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace qsb {
@@ -35,5 +36,8 @@ cudaError_t launch_adjoint_gate2(int dtype, void* psi, void* lam, int n, int q0,
                                  const std::complex<double>* Ud, cudaStream_t s);
 
 int device_sm_count();
+
+// message returned by qs_last_error() on the calling thread (state.cu)
+void set_last_error(const std::string& msg);
 
 }  // namespace qsb

@@ -55,6 +55,14 @@ constexpr uint64_t kBarrierLimitNs = 20ull * 1000ull * 1000ull * 1000ull;  // 20
 
 int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
 
+}  // namespace
+
+namespace qsb {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace qsb
+
+namespace {
+
 // Encode the planned passes after the per-pass scalar extraction (which keeps every gate's
 // planned shape, so the plan made from the original gates stays valid).
 Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& passes, int n, int dtype, int r) {

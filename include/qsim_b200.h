@@ -171,6 +171,22 @@ QS_API int qs_apply_2q_gate(void* psi, int dtype, const void* U, int q0, int q1,
 QS_API int qs_permute_scatter(const void* in, void* out, int dtype, int num_qubits, const int* map_old_to_new,
                        void* stream);
 
+/* Allocation-free gate application (no counterpart in the reference).
+ * For callers that cannot allocate device memory -- code that runs inside a framework
+ * whose allocator already holds the device memory it may use, or that must not trigger the
+ * device-wide synchronisation cudaMalloc/cudaFree imply -- this applies ops (host
+ * matrices, physical bit positions) to a caller-owned device state psi of 2^num_qubits
+ * amplitudes with the same sweep kernel as qs_apply_tile's cooperative mode, and allocates
+ * nothing: its program and grid-barrier words live in one fixed 1 MiB device array that
+ * every GPU loading the library holds until exit.  Calls whose encoded program exceeds that
+ * array (about 20,000 gates) are rejected with an error asking to split them.
+ * The first call on a device looks up the array's device address (with that device
+ * current); make it before any stream capture.  All calls share the array: it is reset at
+ * the start of each call, and calls that overlap on the GPU (other streams, other host
+ * threads) race -- serialise them.  The call returns after the work on `stream` (NULL: the
+ * legacy default stream) has finished. */
+QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_op* ops, int nops, void* stream);
+
 /* Planner inspection (host only, no GPU needed): plan the ops of a tile list for an
  * n-qubit state and report sweeps / phases.  ops use physical bits. */
 QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg,
