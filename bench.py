@@ -416,7 +416,10 @@ def main():
                 "sweeps_per_step": sweeps_step, "reference_sweeps_per_step": len(plan) + R + 1,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved / hbm_peak, "traffic": traffic,
-                             "kernel": "pass_kernel<float,5>", "peak_kind": peak_kind,
+                             "kernel": ("qp_<key>_<pass> (pass kernel specialised at plan time)"
+                                        if st["jit_compile_ms"] or (args.mode == "graphed" and args.jit >= 0 and n >= 20)
+                                        else "pass_kernel<float,5>"),
+                             "peak_kind": peak_kind,
                              "algorithmic_bytes_per_sweep": sweep},
                 "gpu_launches": int(round(launches_step * args.steps)),
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "adjoint": adj}
