@@ -115,6 +115,7 @@ struct Gen {
   std::ostringstream o;
   const float* coef = nullptr;  // interleaved complex64 table
   int nvar = 0;
+  bool used_fa = false;  // the phase accumulated diagonal factors of non-register bits in `fa`
 
   Ent coef_ent(int off) {
     Ent e;
@@ -224,11 +225,11 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         Ent m[4] = {G.coef_ent(c), Gen::cst(0), Gen::cst(0), G.coef_ent(c + 1)};
         G.pairs(g.a, m);
       } else {
-        o << "const float2 d=" << bitcond(g.a - kFixed) << "?LK(" << c + 1 << "):LK(" << c << ");";
-        Ent d;
-        d.cls = 7;
-        d.var = "d";
-        G.scale(d);
+        // a diagonal gate on a non-register bit commutes with every gate of the phase:
+        // its per-thread factor joins the phase's accumulated scalar
+        o << "const float2 d=" << bitcond(g.a - kFixed) << "?LK(" << c + 1 << "):LK(" << c << ");"
+          << "fa=make_float2(fa.x*d.x-fa.y*d.y,fa.x*d.y+fa.y*d.x);";
+        G.used_fa = true;
       }
       break;
     }
@@ -254,11 +255,9 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         G.quads(g.a, g.b, m);
       } else if (fa && fb) {
         o << "const int v=(int)" << bitcond(g.a - kFixed) << "+2*(int)" << bitcond(g.b - kFixed)
-          << ";const float2 d=LK(" << c << "+v);";
-        Ent d;
-        d.cls = 7;
-        d.var = "d";
-        G.scale(d);
+          << ";const float2 d=LK(" << c << "+v);"
+          << "fa=make_float2(fa.x*d.x-fa.y*d.y,fa.x*d.y+fa.y*d.x);";
+        G.used_fa = true;
       } else {
         // one fixed bit selects a diagonal 2x2 on the register bit
         const int J = fa ? g.b : g.a;
@@ -359,8 +358,15 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     for (int h = 0; h < pd.nphase; ++h) {
       const PhaseDesc& ph = phs[pd.phase0 + h];
-      G.o << "case " << h << ":{\n";
+      G.o << "case " << h << ":{\nfloat2 fa=make_float2(1.f,0.f);\n";
+      G.used_fa = false;
       for (int gi = 0; gi < ph.ngate; ++gi) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+      if (G.used_fa) {
+        Ent d;
+        d.cls = 7;
+        d.var = "fa";
+        G.scale(d);
+      }
       G.o << "}break;\n";
     }
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
@@ -467,7 +473,7 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
       std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
       CUfunction f;
       if (d.get_fn(&f, mod, kname) != CUDA_SUCCESS) throw std::runtime_error("jit: kernel not found");
-      if (d.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 200 * 1024) != CUDA_SUCCESS)
+      if (d.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, kMaxDynamicSmem) != CUDA_SUCCESS)
         throw std::runtime_error("jit: cannot raise the shared-memory limit");
       k->functions.push_back(f);
     }

@@ -329,10 +329,10 @@ cudaError_t launch_pass_kernel(int dtype, const uint8_t* d_prog, void* psi, int 
 
 cudaError_t pass_kernel_occupancy(int dtype, int threads, size_t smem, int* blocks_per_sm) {
   if (dtype == 0) {
-    cudaFuncSetAttribute(pass_kernel<float, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(pass_kernel<float, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pass_kernel<float, 5>, threads, smem);
   }
-  cudaFuncSetAttribute(pass_kernel<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(pass_kernel<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, pass_kernel<double, 4>, threads, smem);
 }
 
@@ -379,7 +379,7 @@ template <typename Real, int LR>
 cudaError_t launch_ws(const uint8_t* prog, void* psi, int npass, int threads, size_t smem, unsigned* bar,
                       unsigned* err, uint64_t limit_ns, cudaStream_t stream) {
   auto kern = pass_kernel_ws<Real, LR>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynamicSmem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);

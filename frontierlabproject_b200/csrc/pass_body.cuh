@@ -104,18 +104,18 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 
 constexpr int kPassThreads = 256;
 
-// Issue the asynchronous load of group g into the shared buffer `buf` (16-byte copies,
-// swizzled destinations).  Items: c64 -> two amplitudes (local bit 0 inside the vector),
-// c128 -> one amplitude.
+// Issue the asynchronous load of the group with physical base `gbase` into the shared buffer
+// `buf` (16-byte copies, swizzled destinations).  Items: c64 -> two amplitudes (local bit 0
+// inside the vector), c128 -> one amplitude.  `tbase` = physical offset of this thread's
+// first item.
 template <typename Real>
 __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const typename V2<Real>::T* psi,
-                                               uint64_t g, const PassDesc& pd, const uint64_t* pv, int T, int V) {
+                                               uint64_t gbase, uint64_t tbase, const uint64_t* pv, int T, int V) {
   constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
   const unsigned t = threadIdx.x;
   if ((int)t >= T) return;
-  const uint64_t gbase = group_base(g, pd.gbit, pd.ngbits);
   const uint32_t lt = (uint32_t)t << kItemBits;
-  const uint64_t base = gbase | phys_of_local(lt, pd.sbit, pd.m);
+  const uint64_t base = gbase | tbase;
 #pragma unroll
   for (int v = 0; v < 16; ++v) {
     if (v >= V) break;
@@ -124,10 +124,21 @@ __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const 
   }
 }
 
+// Group index -> physical base: five 7-bit levels of the deposit of g onto the group bits.
+__device__ __forceinline__ uint64_t gbase_of(uint64_t g, const uint64_t* gtab) {
+  return gtab[g & 127] | gtab[128 + ((g >> 7) & 127)] | gtab[256 + ((g >> 14) & 127)] |
+         gtab[384 + ((g >> 21) & 127)] | gtab[512 + ((g >> 28) & 127)];
+}
+
+constexpr int kPhaseTab = 32;   // phases per pass whose thread bases are tabulated
+
 // Exec::run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
 // thread's registers a[] (pb = physical index of the thread's register-0 amplitude).
 // kDouble: two group buffers per block (the next group's copies overlap this group's
 // phases); otherwise one buffer and two resident blocks per SM overlap each other.
+// Index deposits that do not change within a pass (group index -> physical base, thread
+// index -> local/physical base per phase, per-thread load base) are tabulated in shared
+// memory once per pass.
 template <typename Real, int LR, typename Exec, bool kDouble = true>
 __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi,
                                           int pass_begin, int pass_end, unsigned* bar, unsigned* err,
@@ -138,8 +149,14 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
   constexpr int kItemBits = kC64 ? 1 : 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ PassDesc pd;
-  __shared__ uint64_t pv[16];     // physical offset of load/store item row v
-  __shared__ uint32_t sv[16];     // store-permutation source local offset of row v
+  __shared__ uint64_t pv[16];                  // physical offset of load/store item row v
+  __shared__ uint32_t sv[16];                  // store-permutation source local offset of row v
+  __shared__ uint64_t s_gtab[5 * 128];         // group index -> physical base (5 levels x 7 bits)
+  __shared__ uint64_t s_pt[kPhaseTab * 48];    // per phase: physical thread base, t bits 0-3 | 4-8
+  __shared__ uint32_t s_lt[kPhaseTab * 48];    // per phase: local thread base
+  __shared__ uint64_t s_base[512];             // per thread: physical offset of its first item
+  __shared__ uint32_t s_stt[512];              // per thread: store-permutation source of its first item
+  __shared__ uint64_t s_gb[2];                 // physical base of the current group
 
   const unsigned t = threadIdx.x;
   const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
@@ -153,6 +170,7 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
     const int m = pd.m;
     const int T = 1 << (m - pd.r);                    // active threads of this pass
     const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (16)
+    const int nt = m - pd.r;                           // thread-index bits
     for (int v = (int)t; v < V; v += (int)blockDim.x) {
       const uint32_t lv = ((uint32_t)v * (uint32_t)T) << kItemBits;
       uint64_t q = 0;
@@ -165,25 +183,61 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
       pv[v] = q;
       sv[v] = s;
     }
+    for (int e = (int)t; e < 5 * 128; e += (int)blockDim.x) {
+      const int level = e >> 7, idx = e & 127;
+      uint64_t v = 0;
+      for (int j = 0; j < 7; ++j) {
+        const int gb = 7 * level + j;
+        if (gb < pd.ngbits && ((idx >> j) & 1)) v |= 1ull << pd.gbit[gb];
+      }
+      s_gtab[e] = v;
+    }
+    const int nph_tab = pd.nphase < kPhaseTab ? pd.nphase : kPhaseTab;
+    for (int e = (int)t; e < nph_tab * 48; e += (int)blockDim.x) {
+      const int h = e / 48, k = e % 48;
+      const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+      const int lo = k < 16 ? 0 : 4, val = k < 16 ? k : k - 16, nb = k < 16 ? 4 : 5;
+      uint32_t lt = 0;
+      uint64_t pt = 0;
+      for (int b = 0; b < nb; ++b) {
+        const int j = lo + b;
+        if (j < nt && ((val >> b) & 1)) {
+          lt |= 1u << ph->tbit[j];
+          pt |= 1ull << pd.sbit[ph->tbit[j]];
+        }
+      }
+      s_lt[e] = lt;
+      s_pt[e] = pt;
+    }
+    for (int u = (int)t; u < T; u += (int)blockDim.x) {
+      const uint32_t l = (uint32_t)u << kItemBits;
+      s_base[u] = phys_of_local(l, pd.sbit, m);
+      uint32_t st = 0;
+      if (pd.store_perm)
+        for (int j = 0; j < m; ++j) if ((l >> j) & 1u) st |= 1u << pd.store_src[j];
+      s_stt[u] = st;
+    }
     __syncthreads();
     const uint64_t ngroups = 1ull << pd.ngbits;
     const bool active = (int)t < T;
+    const uint64_t tbase = active ? s_base[t] : 0ull;
     C* bufs[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + (kDouble ? (1u << m) : 0u)};
 
     uint64_t g = blockIdx.x;
     if (kDouble) {
-      if (g < ngroups) prefetch_group<Real>(bufs[0], psi, g, pd, pv, T, V);
+      if (g < ngroups) prefetch_group<Real>(bufs[0], psi, gbase_of(g, s_gtab), tbase, pv, T, V);
       cp_async_commit();
     }
     for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
       C* sm = bufs[it & 1];
+      if (t == 0) s_gb[it & 1] = gbase_of(g, s_gtab);  // read after the barrier below
       if (kDouble) {
         const uint64_t gn = g + gridDim.x;
-        if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gn, pd, pv, T, V);
+        if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gbase_of(gn, s_gtab), tbase, pv, T, V);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
-        prefetch_group<Real>(sm, psi, g, pd, pv, T, V);
+        prefetch_group<Real>(sm, psi, gbase_of(g, s_gtab), tbase, pv, T, V);
         cp_async_commit();
         cp_async_wait<0>();
       }
@@ -193,11 +247,13 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
         if (active) {
           const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
           uint32_t sb;
-          uint64_t pb;
-          {
+          uint64_t pb = s_gb[it & 1];
+          if (h < kPhaseTab) {
+            const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
+            sb = swz<Real>(s_lt[e0] | s_lt[e1]);
+            pb |= s_pt[e0] | s_pt[e1];
+          } else {
             uint32_t lb = 0;
-            pb = group_base(g, pd.gbit, pd.ngbits);
-            const int nt = m - pd.r;
             for (int j = 0; j < nt; ++j)
               if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
             sb = swz<Real>(lb);
@@ -229,12 +285,9 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
       }
       // ---- store ----
       if (active) {
-        const uint64_t gbase = group_base(g, pd.gbit, pd.ngbits);
         const uint32_t lt = (uint32_t)t << kItemBits;
-        const uint64_t base = gbase | phys_of_local(lt, pd.sbit, m);
-        uint32_t stt = 0;
-        if (pd.store_perm)
-          for (int j = 0; j < m; ++j) if ((lt >> j) & 1u) stt |= 1u << pd.store_src[j];
+        const uint64_t base = s_gb[it & 1] | s_base[t];
+        const uint32_t stt = s_stt[t];
         if constexpr (kC64) {
 #pragma unroll
           for (int v = 0; v < 16; ++v) {

@@ -213,6 +213,9 @@ namespace {
 struct Scan {
   const std::vector<COp>& ops;
   uint64_t universe;   // bits whose blocking ends the scan
+  // phases: among sets executing equally many gates, prefer those that also hold the
+  // controls and diagonal bits of the executed gates (register renames / half multiplies)
+  bool soft = false;
   // ops (in order) executable with staged set S
   void run(const std::vector<int>& rem, uint64_t S, std::vector<int>& out) const {
     out.clear();
@@ -226,16 +229,16 @@ struct Scan {
     }
   }
   size_t count(const std::vector<int>& rem, uint64_t S) const {
-    size_t c = 0;
+    size_t c = 0, inside = 0;
     uint64_t blocked = 0;
     for (int i : rem) {
       const COp& o = ops[i];
       if (o.touch & blocked) { blocked |= o.touch; }
-      else if ((o.need & ~S) == 0) { ++c; }
+      else if ((o.need & ~S) == 0) { ++c; if ((o.touch & ~S) == 0) ++inside; }
       else { blocked |= o.touch; }
       if ((blocked & universe) == universe) break;
     }
-    return c;
+    return soft ? (c << 8) + inside : c;
   }
 };
 
@@ -292,7 +295,7 @@ static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const 
   uint64_t Smask = 0;
   for (int p : sbits) Smask |= bit(p);
   const int rr = std::min<int>(r, (int)sbits.size());
-  Scan sc{ops, Smask};
+  Scan sc{ops, Smask, true};
   std::vector<PlannedPhase> phases;
   std::vector<int> rem = pass_ops, taken, rest;
   while (!rem.empty()) {
