@@ -313,6 +313,7 @@ def main():
     B.build()
     from frontierlabproject_b200.backend import run_custom_backend
     from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
+    from frontierlabproject_b200.replicas import max_over_ranks, whole_job_rate
 
     hbm_peak, peak_kind = peaks()
     qc, plan, R = build_workload(args.n, args.depth, args.nl, args.seed)
@@ -363,12 +364,9 @@ def main():
     total_ms = start.elapsed_time(end)
     pass_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
     st = sv.stats()
-    if dist:
-        t = torch.tensor([total_ms, pass_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, pass_ms = t.tolist()
+    total_ms, pass_ms = max_over_ranks([total_ms, pass_ms], dist, "cuda")
     ms_step = total_ms / args.steps
-    value = b_alg * world / (ms_step / 1e3) / 1e9
+    value = whole_job_rate(b_alg, ms_step / 1e3, world) / 1e9
     sweeps_step = (st["sweeps"] + st["gate_sweeps"]) / args.steps
     achieved = sweeps_step * sweep / (pass_ms / args.steps / 1e3) / 1e9
     traffic = traffic_from_profile()
@@ -388,13 +386,9 @@ def main():
             _, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode=args.mode, sv=sv,
                                         out=out)
             ts.append(time.perf_counter() - t0)
-        te = float(np.mean(ts))
-        if dist:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = t.item()
+        te, = max_over_ranks([float(np.mean(ts))], dist, "cuda")
         h2d = sum(b.arr.nbytes + sum(k.nbytes for k in b._keep) for _, b in tiles if b is not None)
-        e2e = {"value": b_alg * world / te / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": whole_job_rate(b_alg, te, world) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int((1 << n) * 8), "circuit_time_s": te}
 
     adj = None

@@ -87,11 +87,6 @@ __device__ __forceinline__ uint64_t phys_of_local(uint32_t l, const int8_t* sbit
   for (int j = 0; j < m; ++j) if ((l >> j) & 1u) q |= 1ull << sbit[j];
   return q;
 }
-__device__ __forceinline__ uint64_t group_base(uint64_t g, const int8_t* gbit, int ng) {
-  uint64_t b = 0;
-  for (int j = 0; j < ng; ++j) if ((g >> j) & 1ull) b |= 1ull << gbit[j];
-  return b;
-}
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
