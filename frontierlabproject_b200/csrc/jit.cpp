@@ -116,13 +116,26 @@ struct Gen {
   const float* coef = nullptr;  // interleaved complex64 table
   int nvar = 0;
   bool used_fa = false;  // the phase accumulated diagonal factors of non-register bits in `fa`
+  int kbase = 0, kcount = 0;  // coefficients [kbase, kbase + kcount) arrive as a kernel parameter
+
+  // expression of coefficient `off`: the pass's parameter block (constant bank, an operand
+  // of the arithmetic instruction itself) or, past its capacity, a load from the table
+  std::string kref(int off) const {
+    if (off >= kbase && off < kbase + kcount) return "kp->k[" + std::to_string(off - kbase) + "]";
+    return "LK(" + std::to_string(off) + ")";
+  }
+  // coefficient off + v for a run-time v in [0, n)
+  std::string kref_dyn(int off, int n, const std::string& v) const {
+    if (off >= kbase && off + n <= kbase + kcount) return "kp->k[" + std::to_string(off - kbase) + "+" + v + "]";
+    return "LK(" + std::to_string(off) + "+" + v + ")";
+  }
 
   Ent coef_ent(int off) {
     Ent e;
     e.cls = cls_of(coef[2 * off], coef[2 * off + 1]);
     if (e.cls >= 5) {
       e.var = "k" + std::to_string(nvar++);
-      o << "const float2 " << e.var << " = LK(" << off << ");";
+      o << "const float2 " << e.var << " = " << kref(off) << ";";
     }
     return e;
   }
@@ -196,6 +209,42 @@ struct Gen {
   }
 };
 
+// complex coefficients a gate instruction reads from the table
+int coef_entries(uint8_t kind) {
+  switch (kind) {
+    case GK_1Q_DENSE: case GK_1Q_REAL: case GK_1Q_REIM: case GK_2Q_DIAG: case GK_2Q_CU: return 4;
+    case GK_1Q_DIAG: return 2;
+    case GK_2Q_DENSE: return 16;
+    default: return 0;
+  }
+}
+
+// Coefficients travel as a by-value kernel parameter of each pass kernel (constant bank 0):
+// up to 4000 complex64 entries, 32 000 bytes, within the 32 764-byte parameter limit.
+constexpr int kParamCoefs = 4000;
+
+// The contiguous range of the coefficient table that pass p reads (count capped at
+// kParamCoefs; entries past the cap are loaded from the table).
+void pass_coef_range(const uint8_t* b, int p, int* base, int* count) {
+  const ProgramHeader* hdr = (const ProgramHeader*)b;
+  const PassDesc& pd = ((const PassDesc*)(b + hdr->off_pass))[p];
+  const PhaseDesc* phs = (const PhaseDesc*)(b + hdr->off_phase);
+  const GateInstr* gis = (const GateInstr*)(b + hdr->off_gate);
+  int lo = 0, hi = -1;
+  for (int h = 0; h < pd.nphase; ++h) {
+    const PhaseDesc& ph = phs[pd.phase0 + h];
+    for (int gi = 0; gi < ph.ngate; ++gi) {
+      const GateInstr& g = gis[ph.gate0 + gi];
+      const int ne = coef_entries(g.kind);
+      if (!ne) continue;
+      if (hi < 0 || g.coef < lo) lo = g.coef;
+      hi = std::max(hi, g.coef + ne);
+    }
+  }
+  *base = hi < 0 ? 0 : lo;
+  *count = hi < 0 ? 0 : std::min(hi - lo, kParamCoefs);
+}
+
 std::string bitcond(int phys) { return "((pb>>" + std::to_string(phys) + ")&1ull)"; }
 
 void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& ph) {
@@ -227,7 +276,7 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
       } else {
         // a diagonal gate on a non-register bit commutes with every gate of the phase:
         // its per-thread factor joins the phase's accumulated scalar
-        o << "const float2 d=" << bitcond(g.a - kFixed) << "?LK(" << c + 1 << "):LK(" << c << ");"
+        o << "const float2 d=" << bitcond(g.a - kFixed) << "?" << G.kref(c + 1) << ":" << G.kref(c) << ";"
           << "fa=make_float2(fa.x*d.x-fa.y*d.y,fa.x*d.y+fa.y*d.x);";
         G.used_fa = true;
       }
@@ -255,7 +304,7 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         G.quads(g.a, g.b, m);
       } else if (fa && fb) {
         o << "const int v=(int)" << bitcond(g.a - kFixed) << "+2*(int)" << bitcond(g.b - kFixed)
-          << ";const float2 d=LK(" << c << "+v);"
+          << ";const float2 d=" << G.kref_dyn(c, 4, "v") << ";"
           << "fa=make_float2(fa.x*d.x-fa.y*d.y,fa.x*d.y+fa.y*d.x);";
         G.used_fa = true;
       } else {
@@ -265,8 +314,8 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         // entries indexed b_a + 2 b_b
         const int lo0 = fa ? c + 0 : c + 0, hi0 = fa ? c + 2 : c + 1;   // fixed bit = 0
         const int lo1 = fa ? c + 1 : c + 2, hi1 = fa ? c + 3 : c + 3;   // fixed bit = 1
-        o << "const float2 d0=" << cond << "?LK(" << lo1 << "):LK(" << lo0 << ");const float2 d1=" << cond
-          << "?LK(" << hi1 << "):LK(" << hi0 << ");";
+        o << "const float2 d0=" << cond << "?" << G.kref(lo1) << ":" << G.kref(lo0) << ";const float2 d1=" << cond
+          << "?" << G.kref(hi1) << ":" << G.kref(hi0) << ";";
         Ent m[4];
         m[0].cls = 7; m[0].var = "d0";
         m[3].cls = 7; m[3].var = "d1";
@@ -353,8 +402,10 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
   char kname[64];
   for (int p = pass_begin; p < pass_end; ++p) {
     const PassDesc& pd = pds[p];
-    G.o << "struct X" << p << "{template<typename C,int LR>__device__ __forceinline__ static void run("
-        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb){constexpr int NR=1<<LR;"
+    pass_coef_range(b, p, &G.kbase, &G.kcount);
+    G.o << "struct KP" << p << "{float2 k[" << std::max(1, G.kcount) << "];};\n";
+    G.o << "struct X" << p << "{const KP" << p << "* kp;template<typename C,int LR>__device__ __forceinline__ void run("
+        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
         << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     for (int h = 0; h < pd.nphase; ++h) {
       const PhaseDesc& ph = phs[pd.phase0 + h];
@@ -372,10 +423,13 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
     // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block.  The bound
     // is the block size every pass of the program is launched with (>= this pass's threads).
+    // The pass's coefficients are the by-value parameter kp (constant bank): the arithmetic
+    // reads them as operands, with no load instruction and no register.
     G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ","
-        << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi)"
-        << "{qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
-        << ">(prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
+        << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,"
+        << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};"
+        << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
+        << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
   }
   return G.o.str();
 }
@@ -463,6 +517,9 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
   auto k = std::make_shared<JitKernels>();
   k->key = key;
   k->blocks = cfg.blocks;
+  k->cbase.resize(npass);
+  k->ccount.resize(npass);
+  for (int p = 0; p < npass; ++p) pass_coef_range(prog.bytes.data(), p, &k->cbase[p], &k->ccount[p]);
   Driver& d = driver();
   char kname[64];
   for (int c = 0; c < nchunk; ++c) {
@@ -485,9 +542,12 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
   return k;
 }
 
-cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads,
-                       size_t smem_double, int sms, cudaStream_t stream) {
-  void* args[] = {(void*)&d_prog, (void*)&psi};
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
+                       int threads, size_t smem_double, int sms, cudaStream_t stream) {
+  static const float2 kNone = {0.f, 0.f};
+  // the driver copies the parameter block (the pass's coefficients) at the launch call
+  const void* kp = k.ccount[p] > 0 ? (const void*)((const float2*)host_coef + k.cbase[p]) : (const void*)&kNone;
+  void* args[] = {(void*)&d_prog, (void*)&psi, const_cast<void*>(kp)};
   const unsigned smem = (unsigned)(k.blocks == 1 ? smem_double : smem_double / 2);
   CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)(k.blocks * sms), 1, 1, threads, 1, 1, smem,
                                (CUstream)stream, args, nullptr);

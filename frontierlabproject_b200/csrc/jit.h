@@ -1,9 +1,11 @@
 // Pass kernels specialised at plan time: each pass's register phases become straight-line
 // CUDA (no per-gate dispatch; permutation gates are register renames; zero, +-1, real and
 // imaginary matrix entries skip their multiplies), compiled for sm_100a with NVRTC and
-// loaded as cubins.  Coefficient values stay in the program's table, so a circuit whose
-// parameters change reuses the compiled kernels (the cache key is the program structure
-// plus the zero/one/real/imaginary class of every matrix entry).
+// loaded as cubins.  Coefficient values are not compiled in: each pass kernel receives its
+// range of the coefficient table as a by-value launch parameter (constant bank, read by the
+// arithmetic instructions as operands), so a circuit whose parameters change reuses the
+// compiled kernels (the cache key is the program structure plus the zero/one/real/imaginary
+// class of every matrix entry).
 #pragma once
 #include <memory>
 #include <string>
@@ -25,6 +27,7 @@ struct JitConfig {
 struct JitKernels {
   std::vector<void*> functions;  // CUfunction per pass
   std::vector<void*> modules;    // CUmodule per compiled chunk
+  std::vector<int> cbase, ccount;  // per pass: coefficient-table range passed as its parameter
   uint64_t key = 0;
   int blocks = 1;
   double compile_seconds = 0.0;
@@ -44,9 +47,11 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
 std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
 
 // Launch the specialised kernel of pass p (one launch per pass, no grid barrier).
-// smem_double = bytes of two group buffers (Program::max_smem).
-cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, void* psi, int threads,
-                       size_t smem_double, int sms, cudaStream_t stream);
+// host_coef = the program's coefficient table in host memory: the pass's range of it is
+// copied into the launch's parameter block.  smem_double = bytes of two group buffers
+// (Program::max_smem).
+cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
+                       int threads, size_t smem_double, int sms, cudaStream_t stream);
 
 // Compile a program's source on the host only (tests; returns the NVRTC log on failure).
 bool jit_compile_check(const Program& prog, std::string* log);

@@ -293,7 +293,7 @@ template <typename Real, int LR>
 __global__ void __launch_bounds__(kPassThreads, 1)
 pass_kernel(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi, int pass_begin,
             int pass_end, unsigned* bar, unsigned* err, uint64_t barrier_limit_ns) {
-  pass_body<Real, LR, InterpExec>(prog, psi, pass_begin, pass_end, bar, err, barrier_limit_ns);
+  pass_body<Real, LR, InterpExec>(InterpExec{}, prog, psi, pass_begin, pass_end, bar, err, barrier_limit_ns);
 }
 
 // ------------------------------------------------------------------------------------
@@ -350,7 +350,7 @@ template <typename Real, int LR>
 __global__ void __launch_bounds__(kPassThreads, 1)
 pass_kernel_ws(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi, int pass_begin,
                int pass_end, unsigned* bar, unsigned* err, uint64_t barrier_limit_ns) {
-  pass_body<Real, LR, InterpExec>(prog, psi, pass_begin, pass_end, bar, err, barrier_limit_ns);
+  pass_body<Real, LR, InterpExec>(InterpExec{}, prog, psi, pass_begin, pass_end, bar, err, barrier_limit_ns);
 }
 
 namespace {

@@ -127,7 +127,7 @@ __device__ __forceinline__ uint64_t gbase_of(uint64_t g, const uint64_t* gtab) {
 
 constexpr int kPhaseTab = 32;   // phases per pass whose thread bases are tabulated
 
-// Exec::run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
+// ex.run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
 // thread's registers a[] (pb = physical index of the thread's register-0 amplitude).
 // kDouble: two group buffers per block (the next group's copies overlap this group's
 // phases); otherwise one buffer and two resident blocks per SM overlap each other.
@@ -135,7 +135,8 @@ constexpr int kPhaseTab = 32;   // phases per pass whose thread bases are tabula
 // index -> local/physical base per phase, per-thread load base) are tabulated in shared
 // memory once per pass.
 template <typename Real, int LR, typename Exec, bool kDouble = true>
-__device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, typename V2<Real>::T* __restrict__ psi,
+__device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restrict__ prog,
+                                          typename V2<Real>::T* __restrict__ psi,
                                           int pass_begin, int pass_end, unsigned* bar, unsigned* err,
                                           uint64_t barrier_limit_ns) {
   using C = typename V2<Real>::T;
@@ -264,7 +265,7 @@ __device__ __forceinline__ void pass_body(const uint8_t* __restrict__ prog, type
             for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B[j];
             a[i] = sm[s];
           }
-          Exec::template run<C, LR>(prog, ph, p, h, a, pb);
+          ex.template run<C, LR>(prog, ph, p, h, a, pb);
           opaque(sb);
 #pragma unroll
           for (int j = 0; j < LR; ++j) opaque(B[j]);

@@ -77,9 +77,21 @@ Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& pas
 
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
-  uint64_t key = 0;
+  uint64_t key = 0;        // structure, state and program buffer, grid
+  uint64_t values = 0;     // coefficient values baked into the launch parameters (specialised kernels)
   std::shared_ptr<JitKernels> kernels;
 };
+
+// FNV-1a of the program's coefficient table
+uint64_t coef_values_hash(const Program& prog) {
+  const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = (size_t)hdr->off_coef; i < prog.bytes.size(); ++i) {
+    h ^= prog.bytes[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
 
 struct qs_state {
   int n = 0;
@@ -204,25 +216,51 @@ struct qs_state {
       const uint64_t skey = jk ? jk->key : prog.structure_hash;
       const uint64_t key = skey ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
                            ((uint64_t)(uintptr_t)d_prog << 1) ^ (uint64_t)grid ^ (jk ? 0x5bd1e995ull : 0ull);
-      if (!graph.exec || graph.key != key) {
-        if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
-        graph.kernels = jk;  // keep the modules alive while the graph exists
+      // the specialised kernels take the coefficient values as launch parameters, which the
+      // graph holds: same structure with other values updates the executable graph in place
+      const uint64_t values = jk ? coef_values_hash(prog) : 0;
+      const uint8_t* host_coef = prog.bytes.data() + ((const ProgramHeader*)prog.bytes.data())->off_coef;
+      auto capture = [&]() {
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int p = 0; p < prog.npass && e == cudaSuccess; ++p)
-          e = jk ? jit_launch(*jk, p, d_prog, psi, prog.threads, prog.max_smem, device_sm_count(), stream)
+          e = jk ? jit_launch(*jk, p, d_prog, host_coef, psi, prog.threads, prog.max_smem, device_sm_count(),
+                              stream)
                  : launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false,
                                       d_ctl, d_ctl + 2, kBarrierLimitNs, stream);
         cudaError_t e2 = cudaStreamEndCapture(stream, &g);
         if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
         if (e2 != cudaSuccess) throw CudaError{e2};
+        return g;
+      };
+      bool updated = false;
+      if (graph.exec && graph.key == key && graph.values != values) {
+        cudaGraph_t g = capture();
+        cudaGraphExecUpdateResultInfo info;
+        const cudaError_t eu = cudaGraphExecUpdate(graph.exec, g, &info);
+        cudaGraphDestroy(g);
+        if (eu == cudaSuccess) {
+          graph.values = values;
+          st.graph_builds += 1;
+          updated = true;
+        } else {
+          cudaGetLastError();  // clear the update error; rebuild below
+          CK(cudaGraphExecDestroy(graph.exec));
+          graph.exec = nullptr;
+        }
+      }
+      if (!graph.exec || graph.key != key) {
+        if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
+        graph.kernels = jk;  // keep the modules alive while the graph exists
+        cudaGraph_t g = capture();
         cudaError_t e3 = cudaGraphInstantiate(&graph.exec, g, 0);
         cudaGraphDestroy(g);
         if (e3 != cudaSuccess) throw CudaError{e3};
         graph.key = key;
+        graph.values = values;
         st.graph_builds += 1;
-      } else {
+      } else if (!updated) {
         st.graph_replays += 1;
       }
       CK(cudaGraphLaunch(graph.exec, stream));
