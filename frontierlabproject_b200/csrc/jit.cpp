@@ -468,11 +468,9 @@ std::list<std::shared_ptr<JitKernels>> g_cache;  // most recent first
 
 }  // namespace
 
-bool jit_compile_check(const Program& prog, std::string* log) {
-  std::string why;
+bool jit_compile_check(const Program& prog, std::string* log, const JitConfig& cfg) {
   if (!nvrtc().ok) { if (log) *log = nvrtc().why; return false; }
   const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
-  const JitConfig cfg;
   return compile_source(jit_source(prog, 0, hdr->npass, jit_key(prog, cfg), cfg), nullptr, log, true);
 }
 

@@ -54,6 +54,6 @@ cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const 
                        int threads, size_t smem_double, int sms, cudaStream_t stream);
 
 // Compile a program's source on the host only (tests; returns the NVRTC log on failure).
-bool jit_compile_check(const Program& prog, std::string* log);
+bool jit_compile_check(const Program& prog, std::string* log, const JitConfig& cfg = JitConfig());
 
 }  // namespace qsb

@@ -854,7 +854,10 @@ int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
     for (auto& o : q) c.push_back(classify(o));
-    auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
+    PlanConfig pc = cfg_from(dtype, num_qubits, cfg);
+    // complex64 with an explicit register-bit count: plan as the specialised kernels would
+    if (dtype == 0 && cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) pc.r = cfg->jit_lr;
+    auto passes = plan_passes(c, num_qubits, pc);
     int ph = 0;
     for (auto& p : passes) ph += (int)p.phases.size();
     if (sweeps) *sweeps = (int)passes.size();
@@ -886,7 +889,9 @@ int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cf
     auto passes = plan_passes(c, num_qubits, pc);
     Program prog = build_program(q, passes, num_qubits, 0, pc.r);
     std::string log;
-    const bool ok = jit_compile_check(prog, &log);
+    JitConfig jc;
+    if (cfg && (cfg->jit_blocks == 1 || cfg->jit_blocks == 2)) jc.blocks = cfg->jit_blocks;
+    const bool ok = jit_compile_check(prog, &log, jc);
     if (logbuf && logcap > 0) {
       const size_t k = std::min<size_t>(log.size(), (size_t)logcap - 1);
       std::memcpy(logbuf, log.data(), k);
