@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cstring>
 #include <list>
 #include <mutex>
@@ -140,6 +141,98 @@ struct Gen {
     return e;
   }
   static Ent cst(int cls) { Ent e; e.cls = cls; return e; }
+  Ent cls_ent(int off) const { return cst(cls_of(coef[2 * off], coef[2 * off + 1])); }
+
+  // ---- bit-flip frame of the phase ----
+  // mask[j] names a warp-uniform bool: when true, register index i holds the amplitude of
+  // logical register index i ^ (1 << j).  A bit flip conditioned on a warp-uniform fixed bit
+  // (a CX whose control is a group or warp-index bit) only toggles mask[j]; later gates on
+  // bit j run as their X-conjugated version under the mask, and the phase's stores land at
+  // the flipped addresses.  Empty name: mask known to be false.
+  std::string mask[kMaxR];
+  int nmask = 0;
+  std::ostringstream post;  // declarations emitted after the current gate's block
+  void reset_masks() {
+    for (auto& m : mask) m.clear();
+  }
+  // mask[j] ^= cond (cond: a bool-valued expression)
+  void toggle_mask(int j, const std::string& cond) {
+    const std::string v = "m" + std::to_string(nmask++);
+    post << "const bool " << v << "=" << (mask[j].empty() ? "(bool)(" + cond + ")" : "(" + mask[j] + "!=(bool)(" + cond + "))")
+         << ";";
+    mask[j] = v;
+  }
+  // entries of X^c M X^c for the d x d matrix m (bit k of c flips matrix bit k)
+  static void conjugate(Ent* m, int d, unsigned c) {
+    if (!c) return;
+    Ent t[16];
+    for (int r = 0; r < d; ++r)
+      for (int col = 0; col < d; ++col) t[r * d + col] = m[(r ^ c) * d + (col ^ c)];
+    for (int e = 0; e < d * d; ++e) m[e] = t[e];
+  }
+  // body(c) under every value of the masks of the register bits `bits` (bit k of c = mask of
+  // bits[k]); the versions update the same registers in place
+  void masked(const std::vector<int>& bits, const std::function<void(unsigned)>& body, size_t k = 0,
+              unsigned c = 0) {
+    if (k == bits.size()) {
+      o << "{";
+      body(c);
+      o << "}";
+      return;
+    }
+    if (bits[k] < 0 || bits[k] >= kMaxR || mask[bits[k]].empty()) {
+      masked(bits, body, k + 1, c);
+      return;
+    }
+    o << "if(" << mask[bits[k]] << "){";
+    masked(bits, body, k + 1, c | (1u << k));
+    o << "}else{";
+    masked(bits, body, k + 1, c);
+    o << "}";
+  }
+
+  // Multiplies every entry of the d x d matrix m by the phase factor fa (per-thread values):
+  // the gate then also applies the phase's diagonal factor of its fixed bits.
+  void fold(Ent* m, int d) {
+    static const char* unit[5] = {"", "fa", "make_float2(-fa.x,-fa.y)", "make_float2(-fa.y,fa.x)",
+                                  "make_float2(fa.y,-fa.x)"};
+    for (int e = 0; e < d * d; ++e) {
+      if (m[e].cls == 0) continue;
+      const std::string v = "f" + std::to_string(nvar++);
+      if (m[e].cls <= 4) {
+        o << "const float2 " << v << "=" << unit[m[e].cls] << ";";
+      } else {
+        const std::string& k = m[e].var;
+        o << "const float2 " << v << "=make_float2(fa.x*" << k << ".x-fa.y*" << k << ".y,fa.x*" << k << ".y+fa.y*"
+          << k << ".x);";
+      }
+      m[e].cls = 7;
+      m[e].var = v;
+    }
+  }
+
+  // Arithmetic instructions per amplitude that folding fa into the d x d matrix m adds
+  // (lin's terms: a leading +x is a move, a leading -x / +-ix one instruction per component,
+  // other unit and real/imaginary terms one per component, general terms two).
+  static double fold_added(const Ent* m, int d) {
+    auto term = [](int cls, bool first) {
+      if (cls == 0) return 0;
+      if (cls == 1) return first ? 0 : 2;
+      if (cls <= 4) return first ? 1 : 2;
+      return cls == 7 ? 4 : 2;
+    };
+    double added = 0;
+    for (int r = 0; r < d; ++r) {
+      bool first = true;
+      for (int c = 0; c < d; ++c) {
+        const int cls = m[r * d + c].cls;
+        if (!cls) continue;
+        added += term(7, first) - term(cls, first);
+        first = false;
+      }
+    }
+    return added / d;
+  }
 
   // linear combination sum_c row[c] * x_c; empty string when all terms vanish
   static std::string lin(const Ent* row, const char* const* x, int n) {
@@ -247,7 +340,50 @@ void pass_coef_range(const uint8_t* b, int p, int* base, int* count) {
 
 std::string bitcond(int phys) { return "((pb>>" + std::to_string(phys) + ")&1ull)"; }
 
-void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& ph) {
+// Diagonal gate whose bits are all fixed per thread: a factor of the phase scalar fa.
+bool fixed_diag(const GateInstr& g) {
+  return (g.kind == GK_1Q_DIAG && g.a >= kFixed) || (g.kind == GK_2Q_DIAG && g.a >= kFixed && g.b >= kFixed);
+}
+
+// Entry classes of an unconditional register gate that acts on every amplitude of the thread
+// (so it can absorb the phase scalar); false for other gates.  d = matrix dimension.
+bool absorber_matrix(const Gen& G, const GateInstr& g, Ent* m, int* d) {
+  const int c = g.coef;
+  const bool fa = g.a >= kFixed, fb = g.b >= kFixed;
+  switch (g.kind) {
+    case GK_1Q_DENSE: case GK_1Q_REAL: case GK_1Q_REIM:
+      *d = 2;
+      for (int e = 0; e < 4; ++e) m[e] = G.cls_ent(c + e);
+      return true;
+    case GK_1Q_DIAG:
+      if (fa) return false;
+      *d = 2;
+      m[0] = G.cls_ent(c); m[1] = Gen::cst(0); m[2] = Gen::cst(0); m[3] = G.cls_ent(c + 1);
+      return true;
+    case GK_2Q_DENSE:
+      *d = 4;
+      for (int e = 0; e < 16; ++e) m[e] = G.cls_ent(c + e);
+      return true;
+    case GK_2Q_DIAG:
+      if (fa || fb) return false;
+      *d = 4;
+      for (int e = 0; e < 16; ++e) m[e] = Gen::cst(0);
+      for (int e = 0; e < 4; ++e) m[5 * e] = G.cls_ent(c + e);
+      return true;
+    case GK_2Q_CU:
+      if (fa) return false;
+      *d = 4;
+      for (int r = 0; r < 4; ++r)
+        for (int col = 0; col < 4; ++col) m[4 * r + col] = Gen::cst((r == col && !(r & 1)) ? 1 : 0);
+      m[5] = G.cls_ent(c); m[7] = G.cls_ent(c + 1); m[13] = G.cls_ent(c + 2); m[15] = G.cls_ent(c + 3);
+      return true;
+    default:
+      return false;
+  }
+}
+
+// fold: the gate also applies the phase scalar fa (it must be an absorber_matrix gate)
+void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& ph, bool fold = false) {
   auto& o = G.o;
   o << "{";
   const bool fa = g.a >= kFixed, fb = g.b >= kFixed;
@@ -258,13 +394,33 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
       if (pd.sbit[ph.tbit[j]] == phys) return false;
     return true;
   };
+  // the gate's matrix, X-conjugated under the bit-flip frame of its register operands
+  auto pairs_m = [&](int J, const Ent* m0) {
+    G.masked({J}, [&](unsigned cm) {
+      Ent m[4];
+      std::copy(m0, m0 + 4, m);
+      Gen::conjugate(m, 2, cm);
+      if (fold) G.fold(m, 2);
+      G.pairs(J, m);
+    });
+  };
+  auto quads_m = [&](int A, int B, const Ent* m0) {
+    G.masked({A, B}, [&](unsigned cm) {
+      Ent m[16];
+      std::copy(m0, m0 + 16, m);
+      Gen::conjugate(m, 4, cm);
+      if (fold) G.fold(m, 4);
+      G.quads(A, B, m);
+    });
+  };
   switch (g.kind) {
     case GK_1Q_DENSE: case GK_1Q_REAL: case GK_1Q_REIM: {
       Ent m[4] = {G.coef_ent(c), G.coef_ent(c + 1), G.coef_ent(c + 2), G.coef_ent(c + 3)};
-      G.pairs(g.a, m);
+      pairs_m(g.a, m);
       break;
     }
     case GK_1Q_X: {
+      // register rename; X commutes with the frame
       Ent m[4] = {Gen::cst(0), Gen::cst(1), Gen::cst(1), Gen::cst(0)};
       G.pairs(g.a, m);
       break;
@@ -272,7 +428,7 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
     case GK_1Q_DIAG: {
       if (!fa) {
         Ent m[4] = {G.coef_ent(c), Gen::cst(0), Gen::cst(0), G.coef_ent(c + 1)};
-        G.pairs(g.a, m);
+        pairs_m(g.a, m);
       } else {
         // a diagonal gate on a non-register bit commutes with every gate of the phase:
         // its per-thread factor joins the phase's accumulated scalar
@@ -285,15 +441,17 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
     case GK_2Q_DENSE: {
       Ent m[16];
       for (int e = 0; e < 16; ++e) m[e] = G.coef_ent(c + e);
-      G.quads(g.a, g.b, m);
+      quads_m(g.a, g.b, m);
       break;
     }
     case GK_2Q_SWAP: {
+      // register rename; the frame bits swap with the data
       Ent m[16];
       const int P[4] = {0, 2, 1, 3};
       for (int r = 0; r < 4; ++r)
         for (int col = 0; col < 4; ++col) m[4 * r + col] = Gen::cst(col == P[r] ? 1 : 0);
       G.quads(g.a, g.b, m);
+      std::swap(G.mask[g.a], G.mask[g.b]);
       break;
     }
     case GK_2Q_DIAG: {
@@ -301,7 +459,7 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         Ent m[16];
         for (int e = 0; e < 16; ++e) m[e] = Gen::cst(0);
         for (int e = 0; e < 4; ++e) m[5 * e] = G.coef_ent(c + e);
-        G.quads(g.a, g.b, m);
+        quads_m(g.a, g.b, m);
       } else if (fa && fb) {
         o << "const int v=(int)" << bitcond(g.a - kFixed) << "+2*(int)" << bitcond(g.b - kFixed)
           << ";const float2 d=" << G.kref_dyn(c, 4, "v") << ";"
@@ -319,11 +477,12 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         Ent m[4];
         m[0].cls = 7; m[0].var = "d0";
         m[3].cls = 7; m[3].var = "d1";
-        G.pairs(J, m);
+        pairs_m(J, m);
       }
       break;
     }
     case GK_2Q_CX: case GK_2Q_CU: {
+      if (fold && (g.kind != GK_2Q_CU || fa)) throw std::runtime_error("jit: gate cannot absorb the phase scalar");
       Ent u[4];
       if (g.kind == GK_2Q_CX) {
         u[0] = Gen::cst(0); u[1] = Gen::cst(1); u[2] = Gen::cst(1); u[3] = Gen::cst(0);
@@ -336,15 +495,31 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
         for (int r = 0; r < 4; ++r)
           for (int col = 0; col < 4; ++col) m[4 * r + col] = Gen::cst((r == col && !(r & 1)) ? 1 : 0);
         m[4 * 1 + 1] = u[0]; m[4 * 1 + 3] = u[1]; m[4 * 3 + 1] = u[2]; m[4 * 3 + 3] = u[3];
-        G.quads(g.a, g.b, m);
+        if (g.kind == GK_2Q_CX) {
+          // register rename; a flipped control flips the target's frame bit
+          G.quads(g.a, g.b, m);
+          if (!G.mask[g.a].empty()) G.toggle_mask(g.b, G.mask[g.a]);
+        } else {
+          quads_m(g.a, g.b, m);
+        }
       } else {
         const int P = g.a - kFixed;
-        if (warp_uniform(P)) {
+        if (g.kind == GK_2Q_CX && warp_uniform(P)) {
+          // bit flip under a warp-uniform condition: frame only, no data movement
+          G.toggle_mask(g.b, bitcond(P));
+        } else if (warp_uniform(P)) {
           o << "if(" << bitcond(P) << "){";
-          G.pairs(g.b, u);
+          pairs_m(g.b, u);
           o << "}";
+        } else if (g.kind == GK_2Q_CX) {
+          G.pairs_sel(g.b, u, bitcond(P));  // X commutes with the frame
         } else {
-          G.pairs_sel(g.b, u, bitcond(P));
+          G.masked({g.b}, [&](unsigned cm) {
+            Ent m[4];
+            std::copy(u, u + 4, m);
+            Gen::conjugate(m, 2, cm);
+            G.pairs_sel(g.b, m, bitcond(P));
+          });
         }
       }
       break;
@@ -352,7 +527,8 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
     default:
       throw std::runtime_error("jit: unknown gate kind " + std::to_string((int)g.kind));
   }
-  o << "}\n";
+  o << "}\n" << G.post.str();
+  G.post.str("");
 }
 
 const char* kPrelude = R"(
@@ -404,28 +580,61 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     const PassDesc& pd = pds[p];
     pass_coef_range(b, p, &G.kbase, &G.kcount);
     G.o << "struct KP" << p << "{float2 k[" << std::max(1, G.kcount) << "];};\n";
-    G.o << "struct X" << p << "{const KP" << p << "* kp;template<typename C,int LR>__device__ __forceinline__ void run("
+    G.o << "struct X" << p << "{const KP" << p << "* kp;\n";
+    // swizzled byte offsets of each phase's register bits: immediates
+    G.o << "template<typename Real,int LR>__device__ __forceinline__ void reg_offsets(const qsb::PhaseDesc*,int h,"
+        << "uint32_t (&B)[LR])const{switch(h){";
+    for (int h = 0; h < pd.nphase; ++h) {
+      const PhaseDesc& ph = phs[pd.phase0 + h];
+      G.o << "case " << h << ":";
+      for (int j = 0; j < pd.r; ++j) G.o << "B[" << j << "]=" << swz64(1u << ph.rbit[j]) * 8u << "u;";
+      G.o << "break;";
+    }
+    G.o << "default:break;}}\n";
+    G.o << "template<typename C,int LR>__device__ __forceinline__ uint32_t run("
         << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
         << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     for (int h = 0; h < pd.nphase; ++h) {
       const PhaseDesc& ph = phs[pd.phase0 + h];
       G.o << "case " << h << ":{\nfloat2 fa=make_float2(1.f,0.f);\n";
       G.used_fa = false;
-      for (int gi = 0; gi < ph.ngate; ++gi) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+      G.reset_masks();
+      // Diagonal gates on fixed bits commute with every gate of the phase: their factors
+      // are accumulated first, then folded into the register gate where that costs least
+      // (else one multiply of every amplitude at the end of the phase).
+      for (int gi = 0; gi < ph.ngate; ++gi)
+        if (fixed_diag(gis[ph.gate0 + gi])) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+      int absorber = -1;
       if (G.used_fa) {
+        double best = 4.0;  // instructions per amplitude of the separate multiply
+        for (int gi = 0; gi < ph.ngate; ++gi) {
+          Ent m[16];
+          int d = 0;
+          if (!absorber_matrix(G, gis[ph.gate0 + gi], m, &d)) continue;
+          const double added = Gen::fold_added(m, d);
+          if (added < best) { best = added; absorber = gi; }
+        }
+      }
+      for (int gi = 0; gi < ph.ngate; ++gi)
+        if (!fixed_diag(gis[ph.gate0 + gi])) gen_gate(G, gis[ph.gate0 + gi], pd, ph, gi == absorber);
+      if (G.used_fa && absorber < 0) {
         Ent d;
         d.cls = 7;
         d.var = "fa";
         G.scale(d);
       }
-      G.o << "}break;\n";
+      // local bits left flipped by the phase's bit-flip frame
+      G.o << "return 0u";
+      for (int j = 0; j < pd.r; ++j)
+        if (!G.mask[j].empty()) G.o << "|(" << G.mask[j] << "?" << (1u << ph.rbit[j]) << "u:0u)";
+      G.o << ";}\n";
     }
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
     // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block.  The bound
     // is the block size every pass of the program is launched with (>= this pass's threads).
     // The pass's coefficients are the by-value parameter kp (constant bank): the arithmetic
     // reads them as operands, with no load instruction and no register.
-    G.o << "default:break;}}};\nextern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ","
+    G.o << "default:break;}return 0u;}};\nextern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ","
         << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,"
         << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};"
         << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")

@@ -275,9 +275,14 @@ __device__ __forceinline__ void apply_gate(const GateInstr g, C* a, const C* __r
 // generic pass kernel: gate instructions interpreted from the program
 // ------------------------------------------------------------------------------------
 struct InterpExec {
+  template <typename Real, int LR>
+  __device__ __forceinline__ static void reg_offsets(const PhaseDesc* ph, int, uint32_t (&B8)[LR]) {
+#pragma unroll
+    for (int j = 0; j < LR; ++j) B8[j] = swz<Real>(1u << ph->rbit[j]) * (uint32_t)sizeof(typename V2<Real>::T);
+  }
   template <typename C, int LR>
-  __device__ __forceinline__ static void run(const uint8_t* prog, const PhaseDesc* ph, int, int, C (&a)[1 << LR],
-                                             uint64_t pb) {
+  __device__ __forceinline__ static uint32_t run(const uint8_t* prog, const PhaseDesc* ph, int, int,
+                                                 C (&a)[1 << LR], uint64_t pb) {
     const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
     const GateInstr* gates = reinterpret_cast<const GateInstr*>(prog + hdr->off_gate) + ph->gate0;
     const C* coef = reinterpret_cast<const C*>(prog + hdr->off_coef);
@@ -286,6 +291,7 @@ struct InterpExec {
       const GateInstr gin = gates[gi];
       apply_gate<C, LR>(gin, a, coef, pb);
     }
+    return 0u;  // gates move data in the registers: nothing left flipped
   }
 };
 

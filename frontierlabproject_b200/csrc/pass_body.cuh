@@ -128,7 +128,10 @@ __device__ __forceinline__ uint64_t gbase_of(uint64_t g, const uint64_t* gtab) {
 constexpr int kPhaseTab = 32;   // phases per pass whose thread bases are tabulated
 
 // ex.run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
-// thread's registers a[] (pb = physical index of the thread's register-0 amplitude).
+// thread's registers a[] (pb = physical index of the thread's register-0 amplitude) and
+// returns the local bits left flipped in the registers (the write-back lands at the
+// flipped addresses); ex.reg_offsets(ph, h, B8) gives the swizzled byte offset of each
+// register bit of phase h.
 // kDouble: two group buffers per block (the next group's copies overlap this group's
 // phases); otherwise one buffer and two resident blocks per SM overlap each other.
 // Index deposits that do not change within a pass (group index -> physical base, thread
@@ -217,23 +220,32 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
     const uint64_t ngroups = 1ull << pd.ngbits;
     const bool active = (int)t < T;
     const uint64_t tbase = active ? s_base[t] : 0ull;
-    C* bufs[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + (kDouble ? (1u << m) : 0u)};
+    // Group buffers: buffer 1 starts at byte (esz << m) of the dynamic shared memory, one bit
+    // above every byte offset of a swizzled local index, so a buffer's addresses are XOR
+    // combinations of byte offsets.  Accesses index smem_raw directly (shared-memory
+    // loads/stores with the array base as the immediate offset).
+    constexpr uint32_t kEsz = sizeof(C);
+    const uint32_t buf1 = kDouble ? (kEsz << m) : 0u;
+    auto at = [&](uint32_t byte) -> C& { return *reinterpret_cast<C*>(smem_raw + byte); };
 
     uint64_t g = blockIdx.x;
     if (kDouble) {
-      if (g < ngroups) prefetch_group<Real>(bufs[0], psi, gbase_of(g, s_gtab), tbase, pv, T, V);
+      if (g < ngroups)
+        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, s_gtab), tbase, pv, T, V);
       cp_async_commit();
     }
     for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
-      C* sm = bufs[it & 1];
+      const uint32_t bsel = (it & 1) ? buf1 : 0u;  // byte offset of this group's buffer
       if (t == 0) s_gb[it & 1] = gbase_of(g, s_gtab);  // read after the barrier below
       if (kDouble) {
         const uint64_t gn = g + gridDim.x;
-        if (gn < ngroups) prefetch_group<Real>(bufs[(it & 1) ^ 1], psi, gbase_of(gn, s_gtab), tbase, pv, T, V);
+        if (gn < ngroups)
+          prefetch_group<Real>(reinterpret_cast<C*>(smem_raw + (bsel ^ buf1)), psi, gbase_of(gn, s_gtab), tbase, pv,
+                               T, V);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
-        prefetch_group<Real>(sm, psi, gbase_of(g, s_gtab), tbase, pv, T, V);
+        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, s_gtab), tbase, pv, T, V);
         cp_async_commit();
         cp_async_wait<0>();
       }
@@ -254,27 +266,29 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
               if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
             sb = swz<Real>(lb);
           }
-          uint32_t B[LR];
-#pragma unroll
-          for (int j = 0; j < LR; ++j) B[j] = swz<Real>(1u << ph->rbit[j]);
+          uint32_t sb8 = bsel ^ (sb * kEsz);
+          uint32_t B8[LR];  // byte offset of register bit j (swizzled)
+          ex.template reg_offsets<Real, LR>(ph, h, B8);
           C a[NR];
 #pragma unroll
           for (int i = 0; i < NR; ++i) {
-            uint32_t s = sb;
+            uint32_t s = sb8;
 #pragma unroll
-            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B[j];
-            a[i] = sm[s];
+            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B8[j];
+            a[i] = at(s);
           }
-          ex.template run<C, LR>(prog, ph, p, h, a, pb);
-          opaque(sb);
+          // fl: local bits whose values the phase left flipped in the registers
+          const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
+          sb8 ^= swz<Real>(fl) * kEsz;
+          opaque(sb8);
 #pragma unroll
-          for (int j = 0; j < LR; ++j) opaque(B[j]);
+          for (int j = 0; j < LR; ++j) opaque(B8[j]);
 #pragma unroll
           for (int i = 0; i < NR; ++i) {
-            uint32_t s = sb;
+            uint32_t s = sb8;
 #pragma unroll
-            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B[j];
-            sm[s] = a[i];
+            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B8[j];
+            at(s) = a[i];
           }
         }
         __syncthreads();
@@ -292,11 +306,11 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
             if (pd.store_perm) {
               const uint32_t s0 = stt | sv[v];
               const uint32_t s1 = s0 ^ (1u << pd.store_src[0]);
-              const C x0 = sm[swz<Real>(s0)], x1 = sm[swz<Real>(s1)];
+              const C x0 = at(bsel ^ (swz<Real>(s0) * kEsz)), x1 = at(bsel ^ (swz<Real>(s1) * kEsz));
               val = make_float4(x0.x, x0.y, x1.x, x1.y);
             } else {
               const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << 1);
-              val = *reinterpret_cast<const float4*>(sm + swz<Real>(l));
+              val = *reinterpret_cast<const float4*>(smem_raw + (bsel ^ (swz<Real>(l) * kEsz)));
             }
             __stcg(reinterpret_cast<float4*>(psi + (base | pv[v])), val);
           }
@@ -306,7 +320,7 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
             if (v >= V) break;
             const uint32_t l = lt | ((uint32_t)v * (uint32_t)T);
             const uint32_t src = pd.store_perm ? (stt | sv[v]) : l;
-            __stcg(psi + (base | pv[v]), sm[swz<Real>(src)]);
+            __stcg(psi + (base | pv[v]), at(bsel ^ (swz<Real>(src) * kEsz)));
           }
         }
       }

@@ -90,3 +90,44 @@ def test_jit_parameter_change_reuses_kernels():
         psi, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv,
                                     logical_order=True)
         assert O.infidelity(O.simulate(qc), psi) <= 1e-5
+
+
+def _flip_frame_circuit(n, seed):
+    """Many CX/CY/CU gates whose controls are high qubits (group or warp-index bits of the
+    passes) onto low targets, followed in the same layer by 1q, SWAP, controlled and dense
+    2q gates on those targets: exercises the bit-flip frame of the specialised kernels."""
+    from frontierlabproject_b200.circuit import QuantumCircuit
+    rng = np.random.default_rng(seed)
+    qc = QuantumCircuit(n)
+    lo = list(range(8))
+    hi = list(range(n - 7, n))
+    U = np.linalg.qr(rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4)))[0]
+    for layer in range(10):
+        for q in range(n):
+            [qc.h, qc.sx, qc.x][q % 3](q) if (q + layer) % 2 else qc.rx(float(rng.uniform(0, 6.28)), q)
+        for _ in range(6):
+            qc.cx(int(rng.choice(hi)), int(rng.choice(lo)))
+        a, b = rng.choice(lo, 2, replace=False)
+        qc.cx(int(a), int(b))
+        qc.rz(float(rng.uniform(0, 6.28)), int(b))
+        a, b = rng.choice(lo, 2, replace=False)
+        qc.swap(int(a), int(b))
+        qc.h(int(a))
+        qc.cy(int(rng.choice(hi)), int(rng.choice(lo)))
+        a, b = rng.choice(lo, 2, replace=False)
+        qc.crz(float(rng.uniform(0, 6.28)), int(a), int(b))
+        qc.cp(float(rng.uniform(0, 6.28)), int(rng.choice(hi)), int(rng.choice(lo)))
+        a, b = rng.choice(lo, 2, replace=False)
+        qc.unitary(U, [int(a), int(b)])
+        qc.ry(float(rng.uniform(0, 6.28)), int(a))
+    return qc
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,seed", [(16, 1), (20, 2)])
+def test_jit_flip_frame(n, seed):
+    qc = _flip_frame_circuit(n, seed)
+    psi, _, _, _ = _run_jit(qc, n - 2, logical_order=True)
+    ref = O.simulate(qc)
+    assert O.infidelity(ref, psi) <= 1e-5
+    assert np.max(np.abs(psi - ref)) <= 1e-5
