@@ -269,7 +269,9 @@ def config_of(args, plan, R):
     return {"workload": f"random circuit n={args.n} depth={args.depth} complex64 from |0>, reference LQR "
                         f"schedule nL={args.nl} ({len(plan)} tiles, {R} reorders), seed {args.seed}",
             "n": args.n, "depth": args.depth, "nL": args.nl, "tile_mode": args.mode,
-            "l2": "state (8 GiB at n=30) > L2 (126 MB): every sweep streams from HBM, no flush needed"}
+            "l2": (f"state ({(8 << args.n) / 2**30:g} GiB) > L2 (126 MB): every sweep streams from HBM, "
+                   "no flush needed" if (8 << args.n) > 126e6 else
+                   f"state ({(8 << args.n) / 2**20:g} MiB) fits in L2: not an HBM measurement")}
 
 
 def main():
@@ -288,7 +290,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--jit", type=int, default=0, help="0 auto, 1 always, -1 never")
     ap.add_argument("--jit-lr", type=int, default=5)
-    ap.add_argument("--jit-blocks", type=int, default=1)
+    ap.add_argument("--jit-blocks", type=int, default=2)
     ap.add_argument("--m", type=int, default=13)
     ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()

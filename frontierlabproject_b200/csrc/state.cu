@@ -108,7 +108,8 @@ struct qs_state {
   int grid_mult = 0;
   int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
   int jit_lr = 5;          // register bits per thread of the specialised kernels
-  int jit_blocks = 1;      // resident blocks per SM of the specialised kernels
+  int jit_blocks = 2;      // resident blocks per SM of the specialised kernels (single-buffered
+                           // blocks that overlap each other's group loads)
   // device scratch: program buffer, control words (barrier x2, error), accumulators
   uint8_t* d_prog = nullptr;
   size_t prog_cap = 0;
