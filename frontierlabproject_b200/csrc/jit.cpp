@@ -591,6 +591,16 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       G.o << "break;";
     }
     G.o << "default:break;}}\n";
+    // register bit holding local bit 0 per phase (16-byte pair accesses), -1 if none
+    G.o << "template<int LR>__device__ __forceinline__ int pair_reg(const qsb::PhaseDesc*,int h)const{switch(h){";
+    for (int h = 0; h < pd.nphase; ++h) {
+      const PhaseDesc& ph = phs[pd.phase0 + h];
+      int jr = -1;
+      for (int j = 0; j < pd.r; ++j)
+        if (ph.rbit[j] == 0) jr = j;
+      if (jr >= 0) G.o << "case " << h << ":return " << jr << ";";
+    }
+    G.o << "default:return -1;}}\n";
     G.o << "template<typename C,int LR>__device__ __forceinline__ uint32_t run("
         << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
         << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";

@@ -280,6 +280,13 @@ struct InterpExec {
 #pragma unroll
     for (int j = 0; j < LR; ++j) B8[j] = swz<Real>(1u << ph->rbit[j]) * (uint32_t)sizeof(typename V2<Real>::T);
   }
+  template <int LR>
+  __device__ __forceinline__ static int pair_reg(const PhaseDesc* ph, int) {
+#pragma unroll
+    for (int j = 0; j < LR; ++j)
+      if (ph->rbit[j] == 0) return j;
+    return -1;
+  }
   template <typename C, int LR>
   __device__ __forceinline__ static uint32_t run(const uint8_t* prog, const PhaseDesc* ph, int, int,
                                                  C (&a)[1 << LR], uint64_t pb) {

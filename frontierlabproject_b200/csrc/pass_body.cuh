@@ -127,6 +127,52 @@ __device__ __forceinline__ uint64_t gbase_of(uint64_t g, const uint64_t* gtab) {
 
 constexpr int kPhaseTab = 32;   // phases per pass whose thread bases are tabulated
 
+// Loads (store = false) or stores the thread's 2^LR registers of a phase: register i at byte
+// sb8 ^ (XOR of B8[j] over the set bits j of i).  JR >= 0 (complex64): register bit JR holds
+// local bit 0, so registers i and i | 2^JR are adjacent and move as one 16-byte access (the
+// phase's lanes then span distinct 16-byte slots: no bank conflicts); swap stores the two
+// halves exchanged (local bit 0 left flipped by the phase).
+template <typename C, int LR, int JR>
+__device__ __forceinline__ void regs_io_j(C (&a)[1 << LR], unsigned char* sm, uint32_t sb8, const uint32_t (&B8)[LR],
+                                          bool store, bool swap) {
+#pragma unroll
+  for (int i = 0; i < (1 << LR); ++i) {
+    if (JR >= 0 && ((i >> JR) & 1)) continue;
+    uint32_t s = sb8;
+#pragma unroll
+    for (int j = 0; j < LR; ++j)
+      if (j != JR && ((i >> j) & 1)) s ^= B8[j];
+    if constexpr (JR >= 0) {
+      constexpr int i1 = 1 << (JR < 0 ? 0 : JR);
+      float4* q = reinterpret_cast<float4*>(sm + s);
+      if (store) {
+        const C lo = swap ? a[i | i1] : a[i], hi = swap ? a[i] : a[i | i1];
+        *q = make_float4(lo.x, lo.y, hi.x, hi.y);
+      } else {
+        const float4 v = *q;
+        a[i].x = v.x; a[i].y = v.y;
+        a[i | i1].x = v.z; a[i | i1].y = v.w;
+      }
+    } else {
+      C* q = reinterpret_cast<C*>(sm + s);
+      if (store) *q = a[i];
+      else a[i] = *q;
+    }
+  }
+}
+
+// run-time choice of JR in [J, LR) (or -1)
+template <typename C, int LR, int J>
+__device__ __forceinline__ void regs_io(int jr, C (&a)[1 << LR], unsigned char* sm, uint32_t sb8,
+                                        const uint32_t (&B8)[LR], bool store, bool swap) {
+  if constexpr (J < LR && sizeof(C) == 8) {
+    if (jr == J) { regs_io_j<C, LR, J>(a, sm, sb8, B8, store, swap); return; }
+    regs_io<C, LR, J + 1>(jr, a, sm, sb8, B8, store, swap);
+  } else {
+    regs_io_j<C, LR, -1>(a, sm, sb8, B8, store, swap);
+  }
+}
+
 // ex.run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
 // thread's registers a[] (pb = physical index of the thread's register-0 amplitude) and
 // returns the local bits left flipped in the registers (the write-back lands at the
@@ -269,27 +315,19 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
           uint32_t sb8 = bsel ^ (sb * kEsz);
           uint32_t B8[LR];  // byte offset of register bit j (swizzled)
           ex.template reg_offsets<Real, LR>(ph, h, B8);
+          // register bit holding local bit 0 (complex64): its pairs are 16-byte accesses
+          const int jr = kC64 ? ex.template pair_reg<LR>(ph, h) : -1;
           C a[NR];
-#pragma unroll
-          for (int i = 0; i < NR; ++i) {
-            uint32_t s = sb8;
-#pragma unroll
-            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B8[j];
-            a[i] = at(s);
-          }
+          regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, false, false);
           // fl: local bits whose values the phase left flipped in the registers
           const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
-          sb8 ^= swz<Real>(fl) * kEsz;
+          // a flipped local bit 0 swaps the halves of each 16-byte pair instead
+          const bool swap_pairs = jr >= 0 && (fl & 1u);
+          sb8 ^= swz<Real>(jr >= 0 ? (fl & ~1u) : fl) * kEsz;
           opaque(sb8);
 #pragma unroll
           for (int j = 0; j < LR; ++j) opaque(B8[j]);
-#pragma unroll
-          for (int i = 0; i < NR; ++i) {
-            uint32_t s = sb8;
-#pragma unroll
-            for (int j = 0; j < LR; ++j) if ((i >> j) & 1) s ^= B8[j];
-            at(s) = a[i];
-          }
+          regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, swap_pairs);
         }
         __syncthreads();
       }
