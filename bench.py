@@ -253,6 +253,59 @@ def adjoint_bench(n: int = 24, layers: int = 20, reps: int = 3, seed: int = 0) -
                                   f"x {2 * pc.num_params} per gradient"}
 
 
+def batch_bench(count: int = 512, seed: int = 0, reps: int = 3) -> dict:
+    """Batched variational workload: ``count`` hardware-efficient-ansatz instances (n ~
+    U{12..22}, L ~ U{4..16}, own theta and observable each), energy and full gradient of every
+    instance in one persistent launch, shape chosen by the autotuner; errors against the FP64
+    oracle on a sample of instances; per-instance adjoint engine (one launch per gate) timed on
+    a sample as the comparison."""
+    from frontierlabproject_b200 import circuits as C
+    from frontierlabproject_b200.adjoint import AdjointEngine
+    from frontierlabproject_b200.batch import BatchedAdjoint, BatchShape, autotune, hea_batch
+    from oracle import statevector as O
+    insts = hea_batch(count, seed=seed)
+    t0 = time.perf_counter()
+    shape = autotune(insts, shapes=[BatchShape(13, 13, 4, 256), BatchShape(13, 13, 8, 256),
+                                    BatchShape(12, 12, 4, 256), BatchShape(13, 13, 4, 512)], reps=1)
+    t_tune = time.perf_counter() - t0
+    b = BatchedAdjoint(insts, shape)
+    b.run(timed=True)
+    ms = min(b.run(timed=True) for _ in range(reps))
+    E, G = b.results()
+    # FP64 oracle on the smallest instances
+    order = sorted(range(count), key=lambda i: (insts[i].circuit.num_qubits, len(insts[i].circuit.gates)))[:4]
+    rel = []
+    for i in order:
+        pc = insts[i].circuit
+        L = sum(1 for g in pc.gates if g.name == "ry") // pc.num_qubits
+        E_ref, g_ref = O.adjoint_gradient(C.hea_ansatz(pc.num_qubits, L, insts[i].theta), insts[i].a, insts[i].b)
+        rel.append(float(np.linalg.norm(G[i] - g_ref) / np.linalg.norm(g_ref)))
+    # per-instance engine on a sample (largest and a middle instance), extrapolated by gate count x 2^n
+    sample = [max(range(count), key=lambda i: insts[i].circuit.num_qubits), order[-1]]
+    cost = lambda i: len(insts[i].circuit.gates) * (1 << insts[i].circuit.num_qubits)
+    t_s, c_s = 0.0, 0
+    for i in sample:
+        inst = insts[i]
+        eng = AdjointEngine(inst.circuit.num_qubits, f32=True)
+        eng.energy_and_grad(inst.circuit, inst.theta, inst.a, inst.b)
+        s = time.perf_counter()
+        eng.energy_and_grad(inst.circuit, inst.theta, inst.a, inst.b)
+        t_s += time.perf_counter() - s
+        c_s += cost(i)
+    t_per_inst = t_s * sum(cost(i) for i in range(count)) / c_s
+    info = b.info()
+    nparams = sum(inst.circuit.num_params for inst in insts)
+    return {"workload": f"{count} hardware-efficient-ansatz instances, n ~ U{{12..22}}, L ~ U{{4..16}}, "
+                        f"{nparams} parameters in total, complex64 states, FP64 energies and gradients",
+            "batch_ms": ms, "instances_per_s": count / (ms / 1e3), "parameters_per_s": nparams / (ms / 1e3),
+            "shape": {"m": shape.m, "small_max": shape.small_max, "chunk": shape.chunk, "threads": shape.threads},
+            "autotune_s": t_tune, "work_items": info["items"], "grid": info["grid"],
+            "arena_bytes": info["arena_bytes"], "launches_per_batch": 1,
+            "max_rel_err_vs_fp64_oracle": max(rel), "oracle_sample": [insts[i].circuit.num_qubits for i in order],
+            "per_instance_engine_s_extrapolated": t_per_inst,
+            "speedup_vs_per_instance_engine": t_per_inst / (ms / 1e3)}
+
+
 def choose_cpu_n(n: int) -> int:
     try:
         import psutil
@@ -293,6 +346,7 @@ def main():
     ap.add_argument("--jit-blocks", type=int, default=2)
     ap.add_argument("--m", type=int, default=13)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -396,6 +450,9 @@ def main():
     adj = None
     if not args.no_adjoint:
         adj = adjoint_bench()
+    bat = None
+    if not args.no_batch:
+        bat = batch_bench()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -418,7 +475,7 @@ def main():
                              "peak_kind": peak_kind,
                              "algorithmic_bytes_per_sweep": sweep},
                 "gpu_launches": int(round(launches_step * args.steps)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "adjoint": adj}
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "adjoint": adj, "batch": bat}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -1,0 +1,370 @@
+// Persistent kernel of the batched variational workload (layout and scheduling: batch.h).
+//
+// One launch processes every work item of a batch: blocks take items from a global counter,
+// wait (bounded by a time limit; the error word is set when it runs out) for the items of
+// the same instance's earlier stages, and run them:
+//   SMALL  psi and lam in shared memory: forward sweep, lam = H psi, energy, reverse sweep;
+//   FWD    for each group of the item: stage 2^m amplitudes of psi (16-byte cp.async), apply
+//          the pass's gates in shared memory, store;
+//   HAM    lam = H psi over amplitude chunks (L2 reads of the X-neighbours), energy;
+//   BWD    stage psi and lam, for the pass's gates in reverse: Im <lam|G|psi> (FP64, one
+//          atomic per warp and gate) and psi, lam <- U^dagger psi, lam; store both.
+// Gradients and energies accumulate in FP64; the states are complex64.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "kernels.h"
+
+namespace qsb {
+
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cmac(float2 a, float2 x, float2 b, float2 y) {
+  return make_float2(a.x * x.x - a.y * x.y + b.x * y.x - b.y * y.y, a.x * x.y + a.y * x.x + b.x * y.y + b.y * y.x);
+}
+// Im(conj(l) v), FP64
+__device__ __forceinline__ double im_cv(float2 l, float2 v) { return (double)l.x * v.y - (double)l.y * v.x; }
+
+__device__ __forceinline__ uint64_t gtime() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// every thread of the block calls it (full warps)
+__device__ __forceinline__ void warp_add(double v, double* dst) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dst, v);
+}
+
+__device__ __forceinline__ void cp16(void* smem_dst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+struct Block {
+  BatchItem it;
+  BatchInst in;
+  BatchPass ps;
+  int key;                        // (instance, pass) of the tables below, -1: none
+  int ok;
+  int8_t loc[kBatchMaxQubits];    // local bit of qubit q in the current pass, -1: group bit
+};
+
+// bit of qubit q for local index x of the group with global base gb
+__device__ __forceinline__ int qbit(const int8_t* loc, int q, uint32_t x, uint64_t gb) {
+  const int j = loc[q];
+  return j >= 0 ? (int)((x >> j) & 1u) : (int)((gb >> q) & 1ull);
+}
+
+// 2x2 matrix (m0 m1; m2 m3) on local bit j of A (and of L when kRev); kRev: before the
+// update, acc += Im <L| G |A> on the pair (gen 1 X, 2 Y, 3 Z)
+template <bool kRev>
+__device__ __forceinline__ void pairs2(float2 m0, float2 m1, float2 m2, float2 m3, int gen, float2* A, float2* L,
+                                       int m, int j, double& acc) {
+  const uint32_t half = 1u << (m - 1), lo = (1u << j) - 1u;
+  for (uint32_t k = threadIdx.x; k < half; k += blockDim.x) {
+    const uint32_t i0 = ((k & ~lo) << 1) | (k & lo), i1 = i0 | (1u << j);
+    const float2 p0 = A[i0], p1 = A[i1];
+    A[i0] = cmac(m0, p0, m1, p1);
+    A[i1] = cmac(m2, p0, m3, p1);
+    if (kRev) {
+      const float2 l0 = L[i0], l1 = L[i1];
+      if (gen == 1) acc += im_cv(l0, p1) + im_cv(l1, p0);
+      else if (gen == 2) acc += im_cv(l0, make_float2(p1.y, -p1.x)) + im_cv(l1, make_float2(-p0.y, p0.x));
+      else if (gen == 3) acc += im_cv(l0, p0) - im_cv(l1, p1);
+      L[i0] = cmac(m0, l0, m1, l1);
+      L[i1] = cmac(m2, l0, m3, l1);
+    }
+  }
+}
+
+// One gate on the staged group (forward, or reverse with the gradient slot gslot).
+template <bool kRev>
+__device__ void apply_gate(const BatchGate& g, float2* A, float2* L, int m, uint64_t gb, const int8_t* loc,
+                           double* gslot) {
+  double acc = 0.0;
+  switch (g.kind) {
+    case BG_1Q: {
+      const int j = loc[g.q0];
+      if (!kRev) pairs2<false>(g.u[0], g.u[1], g.u[2], g.u[3], 0, A, L, m, j, acc);
+      else pairs2<true>(cconj(g.u[0]), cconj(g.u[2]), cconj(g.u[1]), cconj(g.u[3]), g.gen, A, L, m, j, acc);
+      break;
+    }
+    case BG_DIAG1: case BG_DIAG2: {
+      const bool two = g.kind == BG_DIAG2;
+      for (uint32_t x = threadIdx.x; x < (1u << m); x += blockDim.x) {
+        const int b0 = qbit(loc, g.q0, x, gb);
+        const int v = two ? b0 + 2 * qbit(loc, g.q1, x, gb) : b0;
+        const float2 d = kRev ? cconj(g.u[v]) : g.u[v];
+        const float2 p = A[x];
+        A[x] = cmul(d, p);
+        if (kRev) {
+          const float2 l = L[x];
+          if (g.gen == 3) acc += b0 ? -im_cv(l, p) : im_cv(l, p);
+          L[x] = cmul(d, l);
+        }
+      }
+      break;
+    }
+    case BG_2Q: {
+      const int j0 = loc[g.q0], j1 = loc[g.q1];
+      auto M = [&](int r, int c) { return kRev ? cconj(g.u[4 * c + r]) : g.u[4 * r + c]; };
+      if (j0 >= 0 && j1 >= 0) {
+        const int lo = j0 < j1 ? j0 : j1, hi = j0 < j1 ? j1 : j0;
+        const uint32_t quarter = 1u << (m - 2);
+        for (uint32_t k = threadIdx.x; k < quarter; k += blockDim.x) {
+          uint32_t base = k & ((1u << lo) - 1u);
+          base |= (k & ((1u << (hi - 1)) - 1u) & ~((1u << lo) - 1u)) << 1;
+          base |= (k & ~((1u << (hi - 1)) - 1u)) << 2;
+          const uint32_t idx[4] = {base, base | (1u << j0), base | (1u << j1), base | (1u << j0) | (1u << j1)};
+          float2 x[4], y[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) { x[c] = A[idx[c]]; if (kRev) y[c] = L[idx[c]]; }
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            float2 s = make_float2(0.f, 0.f), t = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const float2 mc = M(r, c);
+              const float2 a = cmul(mc, x[c]);
+              s.x += a.x; s.y += a.y;
+              if (kRev) { const float2 b = cmul(mc, y[c]); t.x += b.x; t.y += b.y; }
+            }
+            A[idx[r]] = s;
+            if (kRev) L[idx[r]] = t;
+          }
+        }
+      } else if (j0 >= 0 || j1 >= 0) {
+        // block-diagonal in the fixed qubit: the 2x2 block of its value on the staged one
+        if (j1 >= 0) {
+          const int f = (int)((gb >> g.q0) & 1ull);
+          pairs2<kRev>(M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), 0, A, L, m, j1, acc);
+        } else {
+          const int f = (int)((gb >> g.q1) & 1ull);
+          pairs2<kRev>(M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f), M(2 * f + 1, 2 * f + 1), 0, A, L,
+                       m, j0, acc);
+        }
+      }
+      break;
+    }
+    default: break;
+  }
+  if (kRev && g.gen) warp_add(acc, gslot);
+  __syncthreads();
+}
+
+// lam[x] = d(x) psi[x] + sum_i b_i psi[x ^ 2^i] for x in [x0, x1) (psi read through L2 when
+// kGlobal); returns the thread's part of sum Re(conj(psi) lam)
+template <bool kGlobal>
+__device__ __forceinline__ double hamiltonian(const float2* psi, float2* lam, int n, uint64_t x0, uint64_t x1,
+                                              const double* a, const double* b) {
+  double e = 0.0;
+  for (uint64_t x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
+    double d = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const int j = i + 1 == n ? 0 : i + 1;
+      d += (((x >> i) ^ (x >> j)) & 1ull) ? -a[i] : a[i];
+    }
+    const float2 p = kGlobal ? __ldcg(psi + x) : psi[x];
+    double re = d * p.x, im = d * p.y;
+    for (int i = 0; i < n; ++i) {
+      const float2 q = kGlobal ? __ldcg(psi + (x ^ (1ull << i))) : psi[x ^ (1ull << i)];
+      re += b[i] * q.x;
+      im += b[i] * q.y;
+    }
+    const float2 out = make_float2((float)re, (float)im);
+    if (kGlobal) __stcg(lam + x, out);
+    else lam[x] = out;
+    e += (double)p.x * re + (double)p.y * im;
+  }
+  return e;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ prog, float2* __restrict__ arena,
+                                                   double* __restrict__ grads, double* __restrict__ energy,
+                                                   unsigned* __restrict__ ctl, uint64_t limit_ns) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Block B;
+  __shared__ uint64_t s_dep[128 + 64];     // local index -> global offset (bits 0-6 | 7-12)
+  __shared__ uint64_t s_gdep[128 + 128];   // group index -> global offset (bits 0-6 | 7-13)
+  __shared__ double s_coef[2 * kBatchMaxQubits];
+  __shared__ int s_item;
+
+  const BatchHeader* hdr = reinterpret_cast<const BatchHeader*>(prog);
+  const BatchInst* insts = reinterpret_cast<const BatchInst*>(prog + hdr->off_inst);
+  const BatchPass* passes = reinterpret_cast<const BatchPass*>(prog + hdr->off_pass);
+  const BatchGate* gates = reinterpret_cast<const BatchGate*>(prog + hdr->off_gate);
+  const BatchItem* items = reinterpret_cast<const BatchItem*>(prog + hdr->off_item);
+  const double* coef = reinterpret_cast<const double*>(prog + hdr->off_coef);
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* L = A + (1u << hdr->mbuf);
+  const unsigned t = threadIdx.x;
+  if (t == 0) B.key = -1;
+
+  for (;;) {
+    if (t == 0) s_item = (int)atomicAdd(ctl, 1u);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= hdr->nitem) break;
+    // ---- wait for the instance's earlier stages ----
+    if (t == 0) {
+      B.it = items[item];
+      int ok = *(volatile unsigned*)(ctl + 1) == 0u;
+      if (ok && B.it.need > 0) {
+        volatile unsigned* done = ctl + 2 + B.it.inst;
+        const uint64_t t0 = gtime();
+        while (*done < (unsigned)B.it.need) {
+          if (*(volatile unsigned*)(ctl + 1)) { ok = 0; break; }
+          if (gtime() - t0 > limit_ns) { atomicExch(ctl + 1, (unsigned)DERR_BARRIER_TIMEOUT); ok = 0; break; }
+          __nanosleep(128);
+        }
+      }
+      __threadfence();
+      B.ok = ok;
+      const int key = B.it.inst * 4096 + (B.it.kind == BI_HAM ? 4095 : B.it.pass);
+      if (ok && key != B.key) {
+        B.in = insts[B.it.inst];
+        if (B.it.kind != BI_HAM) B.ps = passes[B.in.pass0 + B.it.pass];
+      }
+    }
+    __syncthreads();
+    if (!B.ok) break;
+    const int n = B.in.n;
+    const int key = B.it.inst * 4096 + (B.it.kind == BI_HAM ? 4095 : B.it.pass);
+    if (key != B.key) {
+      // per-pass tables
+      if (B.it.kind != BI_HAM) {
+        const int m = B.ps.m, ng = n - m;
+        if ((int)t < kBatchMaxQubits) B.loc[t] = -1;
+        __syncthreads();
+        if ((int)t < m) B.loc[B.ps.sbit[t]] = (int8_t)t;
+        for (int e = (int)t; e < 128 + 64; e += NT) {
+          const int lvl = e >= 128, v = lvl ? e - 128 : e;
+          uint64_t q = 0;
+          for (int j = 0; j < 7; ++j) {
+            const int lj = 7 * lvl + j;
+            if (lj < m && ((v >> j) & 1)) q |= 1ull << B.ps.sbit[lj];
+          }
+          s_dep[e] = q;
+        }
+        for (int e = (int)t; e < 256; e += NT) {
+          const int lvl = e >= 128, v = lvl ? e - 128 : e;
+          uint64_t q = 0;
+          for (int j = 0; j < 7; ++j) {
+            const int gj = 7 * lvl + j;
+            if (gj < ng && ((v >> j) & 1)) q |= 1ull << B.ps.gbit[gj];
+          }
+          s_gdep[e] = q;
+        }
+      }
+      if ((int)t < 2 * n) s_coef[t] = coef[B.in.coef0 + t];
+      __syncthreads();
+      if (t == 0) B.key = key;
+    }
+    const BatchItem& it = B.it;
+    double* gout = grads + B.in.grad0;
+
+    if (it.kind == BI_SMALL) {
+      const int dim = 1 << n;
+      for (int x = (int)t; x < dim; x += NT) A[x] = make_float2(x == 0 ? 1.f : 0.f, 0.f);
+      __syncthreads();
+      const BatchGate* gs = gates + B.ps.gate0;
+      for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, n, 0, B.loc, nullptr);
+      const double e = hamiltonian<false>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
+      warp_add(e, energy + it.inst);
+      __syncthreads();
+      for (int k = B.ps.ngate - 1; k >= 0; --k) apply_gate<true>(gs[k], A, L, n, 0, B.loc, gout + gs[k].grad);
+    } else if (it.kind == BI_HAM) {
+      const float2* psi = arena + B.in.psi;
+      float2* lam = arena + B.in.lam;
+      const uint64_t chunk = 1ull << B.in.m;
+      const double e = hamiltonian<true>(psi, lam, n, (uint64_t)it.first * chunk,
+                                         (uint64_t)(it.first + it.count) * chunk, s_coef, s_coef + n);
+      warp_add(e, energy + it.inst);
+    } else {
+      const bool rev = it.kind == BI_BWD;
+      const int m = B.ps.m;
+      float2* psi = arena + B.in.psi;
+      float2* lam = arena + B.in.lam;
+      const BatchGate* gs = gates + B.ps.gate0;
+      const uint32_t pairs = 1u << (m - 1);
+      for (int g = it.first; g < it.first + it.count; ++g) {
+        const uint64_t gb = s_gdep[g & 127] | s_gdep[128 + (g >> 7)];
+        if (!rev && it.pass == 0) {
+          for (uint32_t x = t; x < (1u << m); x += NT) A[x] = make_float2((gb == 0 && x == 0) ? 1.f : 0.f, 0.f);
+        } else {
+          for (uint32_t v = t; v < pairs; v += NT) {
+            const uint32_t l = v << 1;
+            const uint64_t off = gb | s_dep[l & 127] | s_dep[128 + (l >> 7)];
+            cp16(A + l, psi + off);
+            if (rev) cp16(L + l, lam + off);
+          }
+          cp_wait_all();
+        }
+        __syncthreads();
+        if (!rev) {
+          for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, m, gb, B.loc, nullptr);
+        } else {
+          for (int k = B.ps.ngate - 1; k >= 0; --k) apply_gate<true>(gs[k], A, L, m, gb, B.loc, gout + gs[k].grad);
+        }
+        for (uint32_t v = t; v < pairs; v += NT) {
+          const uint32_t l = v << 1;
+          const uint64_t off = gb | s_dep[l & 127] | s_dep[128 + (l >> 7)];
+          __stcg(reinterpret_cast<float4*>(psi + off), *reinterpret_cast<const float4*>(A + l));
+          if (rev) __stcg(reinterpret_cast<float4*>(lam + off), *reinterpret_cast<const float4*>(L + l));
+        }
+        __syncthreads();
+      }
+    }
+    // ---- publish completion ----
+    __threadfence();
+    __syncthreads();
+    if (t == 0) atomicAdd(ctl + 2 + it.inst, 1u);
+  }
+}
+
+template <int NT>
+cudaError_t launch_t(const uint8_t* d_prog, void* arena, double* grads, double* energy, unsigned* ctl, int mbuf,
+                     int blocks_per_sm_cap, uint64_t limit_ns, cudaStream_t s, int* grid_out) {
+  const size_t smem = (size_t)2 * (sizeof(float2) << mbuf);
+  auto kern = batch_kernel<NT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  if (blocks_per_sm_cap > 0 && per_sm > blocks_per_sm_cap) per_sm = blocks_per_sm_cap;
+  const int grid = per_sm * device_sm_count();
+  if (grid_out) *grid_out = grid;
+  float2* ar = reinterpret_cast<float2*>(arena);
+  void* args[] = {(void*)&d_prog, (void*)&ar, (void*)&grads, (void*)&energy, (void*)&ctl, (void*)&limit_ns};
+  return cudaLaunchCooperativeKernel((void*)kern, dim3(grid), dim3(NT), args, smem, s);
+}
+
+}  // namespace
+
+cudaError_t launch_batch(const uint8_t* d_prog, void* arena, double* grads, double* energy, unsigned* ctl,
+                         int threads, int mbuf, int blocks_per_sm_cap, uint64_t limit_ns, cudaStream_t s,
+                         int* grid_out) {
+  if (mbuf < 1 || mbuf > kBatchMaxLocal) return cudaErrorInvalidValue;
+  if (threads == 512)
+    return launch_t<512>(d_prog, arena, grads, energy, ctl, mbuf, blocks_per_sm_cap, limit_ns, s, grid_out);
+  if (threads == 256)
+    return launch_t<256>(d_prog, arena, grads, energy, ctl, mbuf, blocks_per_sm_cap, limit_ns, s, grid_out);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace qsb

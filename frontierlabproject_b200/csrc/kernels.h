@@ -35,6 +35,11 @@ cudaError_t launch_adjoint_gate1(int dtype, void* psi, void* lam, int n, int q, 
 cudaError_t launch_adjoint_gate2(int dtype, void* psi, void* lam, int n, int q0, int q1,
                                  const std::complex<double>* Ud, cudaStream_t s);
 
+// batched variational workload (kern_batch.cu): one cooperative persistent launch
+cudaError_t launch_batch(const uint8_t* d_prog, void* arena, double* grads, double* energy, unsigned* ctl,
+                         int threads, int mbuf, int blocks_per_sm_cap, uint64_t limit_ns, cudaStream_t s,
+                         int* grid_out);
+
 int device_sm_count();
 
 // message returned by qs_last_error() on the calling thread (state.cu)

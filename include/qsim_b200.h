@@ -203,6 +203,46 @@ QS_API int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_con
 QS_API int qs_perm_emulate(int num_qubits, int dtype, const int* perm, const qs_config* cfg, void* psi,
                     int* sweeps);
 
+/* ---- Batched variational workload (no counterpart in the reference executor) ----------
+ * Energy E_i = <psi_i|H_i|psi_i> and the full adjoint gradient dE_i/dtheta of many
+ * independent circuits of uneven qubit count, in ONE persistent cooperative launch per
+ * batch: psi_i = U_i |0...0> (complex64), H_i = sum_j a_j Z_j Z_{(j+1) mod n} + b_j X_j,
+ * FP64 energies and gradients.  Instances up to small_max qubits run entirely in shared
+ * memory; larger ones stream their states from an HBM arena in planned passes. */
+typedef struct qs_batch qs_batch;
+typedef struct {
+  int num_qubits;       /* 2 .. 26 */
+  const qs_adj_op* ops; /* the circuit (qubit indices = bit positions); gen marks rotations */
+  int nops;
+  int nparams;          /* gradient slots: grad_index < nparams */
+  const double* a;      /* observable coefficients, num_qubits each */
+  const double* b;
+} qs_batch_instance;
+typedef struct {
+  int m;             /* staged bits per group of the arena instances (9 .. 13) */
+  int small_max;     /* instances with num_qubits <= small_max run in shared memory (0 .. 13) */
+  int chunk;         /* groups per work item (>= 1) */
+  int threads;       /* threads per block: 256 or 512 */
+  int blocks_per_sm; /* cap on resident blocks per SM (0: as many as fit) */
+} qs_batch_config;
+/* Plan and encode the batch, allocate its device program, arena and outputs (cfg NULL:
+ * m 13, small_max 13, chunk 4, 256 threads). */
+QS_API int qs_batch_create(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, qs_batch** out);
+/* New gate matrices / observables for the same instance shapes (re-encodes the program). */
+QS_API int qs_batch_set_params(qs_batch* b, const qs_batch_instance* insts, int ninst);
+/* Launch the batch on stream (NULL: legacy default stream).  ms (optional): device time of
+ * the launch, waiting for it. */
+QS_API int qs_batch_run(qs_batch* b, void* stream, float* ms);
+/* Wait for the device, then copy energies (ninst) and gradients (concatenated in instance
+ * order, nparams each); QS_ERR_DEVICE when a dependency wait of the kernel timed out. */
+QS_API int qs_batch_results(qs_batch* b, double* energies, double* grads);
+QS_API int qs_batch_info(const qs_batch* b, int* nitems, int* nparams_total, long long* arena_bytes, int* grid);
+QS_API int qs_batch_destroy(qs_batch* b);
+/* Host emulation of the same device program (items in list order, FP64 states): tests of
+ * the batch planner and encoder without a GPU. */
+QS_API int qs_batch_emulate(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, double* energies,
+                            double* grads);
+
 #ifdef __cplusplus
 }
 #endif
