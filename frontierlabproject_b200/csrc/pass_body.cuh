@@ -327,7 +327,8 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
           opaque(sb8);
 #pragma unroll
           for (int j = 0; j < LR; ++j) opaque(B8[j]);
-          regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, swap_pairs);
+          if (swap_pairs) regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, true);  // warp-uniform
+          else regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, false);
         }
         __syncthreads();
       }
