@@ -40,6 +40,13 @@ cudaError_t launch_batch(const uint8_t* d_prog, void* arena, double* grads, doub
                          int threads, int mbuf, int blocks_per_sm_cap, uint64_t limit_ns, cudaStream_t s,
                          int* grid_out);
 
+// dense 64x64 unitary on the six lowest qubits on the tensor cores (kern_dense_tc.cu):
+// weights = dense6_weight_bytes() bytes prepared by dense6_prepare_weights (device copy)
+size_t dense6_weight_bytes();
+void dense6_prepare_weights(const std::complex<double>* U, uint8_t* out);
+cudaError_t launch_dense6_tc(void* psi, int n, const void* d_weights, unsigned* err, uint64_t limit_ns,
+                             cudaStream_t s);
+
 int device_sm_count();
 
 // message returned by qs_last_error() on the calling thread (state.cu)

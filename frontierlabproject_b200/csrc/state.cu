@@ -127,9 +127,11 @@ struct qs_state {
   GraphEntry graph;
   std::vector<std::pair<uint64_t, std::pair<size_t, std::vector<PlannedPass>>>> plan_cache;
   qs_stats st{};
+  void* d_dense = nullptr;    // tensor-core operand of the last dense 6-qubit unitary
 
   ~qs_state() {
     if (graph.exec) cudaGraphExecDestroy(graph.exec);
+    if (d_dense) cudaFree(d_dense);
     if (psi) cudaFree(psi);
     if (d_prog) cudaFree(d_prog);
     for (Slot& s : slots) {
@@ -626,6 +628,34 @@ int qs_flush(qs_state* s) {
 
 int qs_materialize(qs_state* s) {
   return guard([&] { if (!s) throw InvalidArg{"null state"}; s->materialize(); });
+}
+
+int qs_dense6_weights(const double* U, void* out) {
+  return guard([&] {
+    if (!U || !out) throw InvalidArg{"null argument"};
+    std::vector<cplx> u(4096);
+    for (int i = 0; i < 4096; ++i) u[i] = cplx(U[2 * i], U[2 * i + 1]);
+    dense6_prepare_weights(u.data(), (uint8_t*)out);
+  });
+}
+
+int qs_apply_dense6(qs_state* s, const double* U) {
+  return guard([&] {
+    if (!s || !U) throw InvalidArg{"null argument"};
+    if (s->dtype != 0) throw InvalidArg{"apply_dense6: complex64 states only"};
+    if (s->n < 13) throw InvalidArg{"apply_dense6: needs at least 13 qubits"};
+    s->materialize();  // queued gates first; layout positions 0..5 become physical bits 0..5
+    std::vector<cplx> u(4096);
+    for (int i = 0; i < 4096; ++i) u[i] = cplx(U[2 * i], U[2 * i + 1]);
+    std::vector<uint8_t> w(dense6_weight_bytes());
+    dense6_prepare_weights(u.data(), w.data());
+    if (!s->d_dense) CK(cudaMalloc(&s->d_dense, w.size()));
+    // pageable source: staged before the call returns, copied in stream order
+    CK(cudaMemcpyAsync(s->d_dense, w.data(), w.size(), cudaMemcpyHostToDevice, s->stream));
+    CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, kBarrierLimitNs, s->stream));
+    s->st.launches += 1;
+    s->st.gate_sweeps += 1;
+  });
 }
 
 int qs_device_ptr(qs_state* s, void** out) {

@@ -178,6 +178,27 @@ class _StatevectorBase:
         """Launch queued ops and the data movement to the current layout (asynchronous)."""
         N.call("qs_materialize", self._h)
 
+    def apply_dense(self, U, qubits: Sequence[int] = (0, 1, 2, 3, 4, 5)) -> None:
+        """Dense 64x64 unitary on six layout positions in one tensor-core sweep (complex64,
+        >= 13 qubits); row/column index sum_j b_{qubits[j]} 2^j.  Other positions are first
+        relabelled onto 0..5 (and back), which costs in-place permutation sweeps."""
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        if U.shape != (64, 64):
+            raise RuntimeError("U must be a 64x64 matrix")
+        q = [int(x) for x in qubits]
+        n = self.num_qubits
+        if len(q) != 6 or len(set(q)) != 6 or any(x < 0 or x >= n for x in q):
+            raise RuntimeError("apply_dense: six distinct qubit positions required")
+        if q == list(range(6)):
+            N.call("qs_apply_dense6", self._h, U.ctypes.data)
+            return
+        # label each position by itself; the new layout lists q first (positions 0..5)
+        ident = list(range(n))
+        moved = q + [p for p in range(n) if p not in q]
+        self.permute(ident, moved)
+        N.call("qs_apply_dense6", self._h, U.ctypes.data)
+        self.permute(moved, ident)
+
     # -- layout ------------------------------------------------------------------------
     def permute(self, layout_old: Sequence[int], layout_new: Sequence[int]) -> None:
         n = self.num_qubits

@@ -120,6 +120,17 @@ QS_API int qs_apply_diagonal_1q(qs_state* s, int target_qubit, const double* pha
 QS_API int qs_flush(qs_state* s);
 /* Run queued ops and move the data to the current layout (asynchronously). */
 QS_API int qs_materialize(qs_state* s);
+/* Dense 64x64 unitary on layout positions 0..5 (no counterpart in the reference executor;
+ * the k=6 fused-gate form of the north-star design): U is a host complex128 matrix, row-major,
+ * row/column index sum_j b_j 2^j over positions j = 0..5.  Complex64 states of >= 13 qubits.
+ * One sweep on the tensor cores (tcgen05 MMAs, operands split into BF16 high and low parts,
+ * FP32 accumulation in tensor memory); queued gates run first and the layout is materialised. */
+QS_API int qs_apply_dense6(qs_state* s, const double* U);
+/* The tensor-core operand qs_apply_dense6 builds from U (host only; 65536 bytes into out):
+ * the 128x128 real form W (row 2r+q, column 2s+p: q,p = 0 real / 1 imaginary part) split into
+ * BF16 high and low parts, in the canonical K-major layout (8-row x 16-byte core matrices,
+ * K-chunks 128 B apart, 8-row groups 2048 B apart), high part first. */
+QS_API int qs_dense6_weights(const double* U, void* out);
 /* Device address of the amplitudes in the current layout (executes queued ops and
  * pending data movement, then synchronises).  Valid until the next call on s. */
 QS_API int qs_device_ptr(qs_state* s, void** out);
