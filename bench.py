@@ -390,6 +390,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=512, help="instances of the batched variational workload")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -495,7 +496,7 @@ def main():
         adj = adjoint_bench()
     bat = None
     if not args.no_batch:
-        bat = batch_bench()
+        bat = batch_bench(args.batch_count)
     den = None
     if not args.no_dense:
         den = dense_bench(n)
