@@ -67,11 +67,14 @@ __device__ __forceinline__ int qbit(const int8_t* loc, int q, uint32_t x, uint64
   return j >= 0 ? (int)((x >> j) & 1u) : (int)((gb >> q) & 1ull);
 }
 
-// 2x2 matrix (m0 m1; m2 m3) on local bit j of A (and of L when kRev); kRev: before the
-// update, acc += Im <L| G |A> on the pair (gen 1 X, 2 Y, 3 Z)
-template <bool kRev>
-__device__ __forceinline__ void pairs2(float2 m0, float2 m1, float2 m2, float2 m3, int gen, float2* A, float2* L,
-                                       int m, int j, double& acc) {
+// Im(conj(l) v) in FP32 (per-pair gradient terms; each thread's sum is reduced in FP64)
+__device__ __forceinline__ float im_cvf(float2 l, float2 v) { return l.x * v.y - l.y * v.x; }
+
+// 2x2 matrix (m0 m1; m2 m3) on local bit j of A (and of L when kRev); kRev with GEN != 0:
+// before the update, acc += Im <L| G |A> on the pair (GEN 1 X, 2 Y, 3 Z)
+template <bool kRev, int GEN>
+__device__ __forceinline__ void pairs2g(float2 m0, float2 m1, float2 m2, float2 m3, float2* A, float2* L, int m, int j,
+                                        float& acc) {
   const uint32_t half = 1u << (m - 1), lo = (1u << j) - 1u;
   for (uint32_t k = threadIdx.x; k < half; k += blockDim.x) {
     const uint32_t i0 = ((k & ~lo) << 1) | (k & lo), i1 = i0 | (1u << j);
@@ -80,46 +83,79 @@ __device__ __forceinline__ void pairs2(float2 m0, float2 m1, float2 m2, float2 m
     A[i1] = cmac(m2, p0, m3, p1);
     if (kRev) {
       const float2 l0 = L[i0], l1 = L[i1];
-      if (gen == 1) acc += im_cv(l0, p1) + im_cv(l1, p0);
-      else if (gen == 2) acc += im_cv(l0, make_float2(p1.y, -p1.x)) + im_cv(l1, make_float2(-p0.y, p0.x));
-      else if (gen == 3) acc += im_cv(l0, p0) - im_cv(l1, p1);
+      if (GEN == 1) acc += im_cvf(l0, p1) + im_cvf(l1, p0);
+      if (GEN == 2) acc += im_cvf(l0, make_float2(p1.y, -p1.x)) + im_cvf(l1, make_float2(-p0.y, p0.x));
+      if (GEN == 3) acc += im_cvf(l0, p0) - im_cvf(l1, p1);
       L[i0] = cmac(m0, l0, m1, l1);
       L[i1] = cmac(m2, l0, m3, l1);
     }
   }
 }
 
-// One gate on the staged group (forward, or reverse with the gradient slot gslot).
 template <bool kRev>
-__device__ void apply_gate(const BatchGate& g, float2* A, float2* L, int m, uint64_t gb, const int8_t* loc,
+__device__ __forceinline__ void pairs2(float2 m0, float2 m1, float2 m2, float2 m3, int gen, float2* A, float2* L,
+                                       int m, int j, float& acc) {
+  if (!kRev || gen == 0) pairs2g<kRev, 0>(m0, m1, m2, m3, A, L, m, j, acc);
+  else if (gen == 1) pairs2g<kRev, 1>(m0, m1, m2, m3, A, L, m, j, acc);
+  else if (gen == 2) pairs2g<kRev, 2>(m0, m1, m2, m3, A, L, m, j, acc);
+  else pairs2g<kRev, 3>(m0, m1, m2, m3, A, L, m, j, acc);
+}
+
+// Diagonal gate: entry d[b0 + 2 b1] per amplitude, the bits taken from the local index (jq >= 0)
+// or fixed by the group (jq < 0: value fq).  kZ: acc += Im <L|Z_q0|A> before the update.
+template <bool kRev, bool kZ>
+__device__ __forceinline__ void diag_g(float2 d0, float2 d1, float2 d2, float2 d3, int j0, int f0, int j1, int f1,
+                                       float2* A, float2* L, int m, float& acc) {
+  for (uint32_t x = threadIdx.x; x < (1u << m); x += blockDim.x) {
+    const int b0 = j0 >= 0 ? (int)((x >> j0) & 1u) : f0;
+    const int b1 = j1 >= 0 ? (int)((x >> j1) & 1u) : f1;
+    const float2 d = b1 ? (b0 ? d3 : d2) : (b0 ? d1 : d0);
+    const float2 p = A[x];
+    A[x] = cmul(d, p);
+    if (kRev) {
+      const float2 l = L[x];
+      if (kZ) acc += b0 ? -im_cvf(l, p) : im_cvf(l, p);
+      L[x] = cmul(d, l);
+    }
+  }
+}
+
+// One gate on the staged group (forward, or reverse with the gradient slot gslot).  The gate's
+// fields are read once into registers (the loops touch only shared memory).
+template <bool kRev>
+__device__ void apply_gate(const BatchGate& gref, float2* A, float2* L, int m, uint64_t gb, const int8_t* loc,
                            double* gslot) {
-  double acc = 0.0;
-  switch (g.kind) {
+  float acc = 0.0f;
+  const int kind = gref.kind, q0 = gref.q0, q1 = gref.q1, gen = gref.gen;
+  switch (kind) {
     case BG_1Q: {
-      const int j = loc[g.q0];
-      if (!kRev) pairs2<false>(g.u[0], g.u[1], g.u[2], g.u[3], 0, A, L, m, j, acc);
-      else pairs2<true>(cconj(g.u[0]), cconj(g.u[2]), cconj(g.u[1]), cconj(g.u[3]), g.gen, A, L, m, j, acc);
+      const float2 u0 = gref.u[0], u1 = gref.u[1], u2 = gref.u[2], u3 = gref.u[3];
+      const int j = loc[q0];
+      if (!kRev) pairs2<false>(u0, u1, u2, u3, 0, A, L, m, j, acc);
+      else pairs2<true>(cconj(u0), cconj(u2), cconj(u1), cconj(u3), gen, A, L, m, j, acc);
       break;
     }
     case BG_DIAG1: case BG_DIAG2: {
-      const bool two = g.kind == BG_DIAG2;
-      for (uint32_t x = threadIdx.x; x < (1u << m); x += blockDim.x) {
-        const int b0 = qbit(loc, g.q0, x, gb);
-        const int v = two ? b0 + 2 * qbit(loc, g.q1, x, gb) : b0;
-        const float2 d = kRev ? cconj(g.u[v]) : g.u[v];
-        const float2 p = A[x];
-        A[x] = cmul(d, p);
-        if (kRev) {
-          const float2 l = L[x];
-          if (g.gen == 3) acc += b0 ? -im_cv(l, p) : im_cv(l, p);
-          L[x] = cmul(d, l);
-        }
+      const bool two = kind == BG_DIAG2;
+      float2 d[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 v = (two || e < 2) ? gref.u[two ? e : (e & 1)] : make_float2(0.f, 0.f);
+        d[e] = kRev ? cconj(v) : v;
       }
+      if (!two) { d[2] = d[0]; d[3] = d[1]; }
+      const int j0 = loc[q0], f0 = (int)((gb >> q0) & 1ull);
+      const int j1 = two ? loc[q1] : -1, f1 = two ? (int)((gb >> q1) & 1ull) : 0;
+      if (kRev && gen == 3) diag_g<kRev, true>(d[0], d[1], d[2], d[3], j0, f0, j1, f1, A, L, m, acc);
+      else diag_g<kRev, false>(d[0], d[1], d[2], d[3], j0, f0, j1, f1, A, L, m, acc);
       break;
     }
     case BG_2Q: {
-      const int j0 = loc[g.q0], j1 = loc[g.q1];
-      auto M = [&](int r, int c) { return kRev ? cconj(g.u[4 * c + r]) : g.u[4 * r + c]; };
+      const int j0 = loc[q0], j1 = loc[q1];
+      float2 u[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) u[e] = gref.u[e];
+      auto M = [&](int r, int c) { return kRev ? cconj(u[4 * c + r]) : u[4 * r + c]; };
       if (j0 >= 0 && j1 >= 0) {
         const int lo = j0 < j1 ? j0 : j1, hi = j0 < j1 ? j1 : j0;
         const uint32_t quarter = 1u << (m - 2);
@@ -148,10 +184,10 @@ __device__ void apply_gate(const BatchGate& g, float2* A, float2* L, int m, uint
       } else if (j0 >= 0 || j1 >= 0) {
         // block-diagonal in the fixed qubit: the 2x2 block of its value on the staged one
         if (j1 >= 0) {
-          const int f = (int)((gb >> g.q0) & 1ull);
+          const int f = (int)((gb >> q0) & 1ull);
           pairs2<kRev>(M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), 0, A, L, m, j1, acc);
         } else {
-          const int f = (int)((gb >> g.q1) & 1ull);
+          const int f = (int)((gb >> q1) & 1ull);
           pairs2<kRev>(M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f), M(2 * f + 1, 2 * f + 1), 0, A, L,
                        m, j0, acc);
         }
@@ -160,7 +196,7 @@ __device__ void apply_gate(const BatchGate& g, float2* A, float2* L, int m, uint
     }
     default: break;
   }
-  if (kRev && g.gen) warp_add(acc, gslot);
+  if (kRev && gen) warp_add((double)acc, gslot);
   __syncthreads();
 }
 
