@@ -27,8 +27,6 @@ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y
 __device__ __forceinline__ float2 cmac(float2 a, float2 x, float2 b, float2 y) {
   return make_float2(a.x * x.x - a.y * x.y + b.x * y.x - b.y * y.y, a.x * x.y + a.y * x.x + b.x * y.y + b.y * y.x);
 }
-// Im(conj(l) v), FP64
-__device__ __forceinline__ double im_cv(float2 l, float2 v) { return (double)l.x * v.y - (double)l.y * v.x; }
 
 __device__ __forceinline__ uint64_t gtime() {
   uint64_t t;
@@ -60,12 +58,6 @@ struct Block {
   int ok;
   int8_t loc[kBatchMaxQubits];    // local bit of qubit q in the current pass, -1: group bit
 };
-
-// bit of qubit q for local index x of the group with global base gb
-__device__ __forceinline__ int qbit(const int8_t* loc, int q, uint32_t x, uint64_t gb) {
-  const int j = loc[q];
-  return j >= 0 ? (int)((x >> j) & 1u) : (int)((gb >> q) & 1ull);
-}
 
 // Im(conj(l) v) in FP32 (per-pair gradient terms; each thread's sum is reduced in FP64)
 __device__ __forceinline__ float im_cvf(float2 l, float2 v) { return l.x * v.y - l.y * v.x; }

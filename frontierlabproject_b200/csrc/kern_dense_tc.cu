@@ -8,15 +8,17 @@
 //     D = X^T W^T,  D[c][2r+q] = (U x_c)_r re/im,
 // computed as X_hi W_hi + X_hi W_lo + X_lo W_hi with both operands split into BF16 high and
 // low parts (about 16 significant bits each), FP32 accumulation in tensor memory.  Row c of D
-// is the new column c in memory order, so each thread stores its column contiguously.
+// is the new column c in memory order: each thread moves its row into a staging buffer, then
+// every warp stores whole 512-byte columns (coalesced).
 //
 // Operands are in shared memory in the canonical K-major layout without swizzle: core
 // matrices of 8 rows x 16 bytes, K-chunks 128 B apart, 8-row groups 2048 B apart.  One thread
 // per warpgroup issues the MMAs (M=128, N=128, K=16, 8 K-steps x 3 products) and commits them
-// to an mbarrier; the warpgroup waits (bounded), reads its accumulator rows with tcgen05.ld and
-// stores.  Two warpgroups per block work on alternate tiles (own operand buffer, own TMEM
-// columns, own named barrier); W is shared.  Waits are bounded by a time limit; on expiry the
-// error word is set and the block frees its tensor memory and returns.
+// to an mbarrier; after a bounded wait the block reads its accumulator rows with tcgen05.ld.
+// One warpgroup (128 threads) per block and SM: while a tile is converted, multiplied and
+// written back, the next tile's columns are already on their way into a staging buffer
+// (16-byte cp.async, a warp per column: coalesced).  Waits are bounded by a time limit; on
+// expiry the error word is set and the block frees its tensor memory and returns.
 #include <complex>
 #include <cstdint>
 #include <cstring>
@@ -29,11 +31,7 @@ namespace qsb {
 
 namespace {
 
-constexpr int kWG = 2;                       // warpgroups per block
-constexpr int kThreadsTC = 128 * kWG;
 constexpr uint32_t kOp = 128 * 128 * 2;      // one BF16 operand (128 rows x 128 K): 32 KiB
-constexpr uint32_t kSmemTC = 2 * kOp + kWG * 2 * kOp;  // W hi/lo + per warpgroup X hi/lo = 192 KiB
-constexpr uint32_t kTmemCols = 128 * kWG;
 
 __device__ __forceinline__ uint64_t gtime_tc() {
   uint64_t t;
@@ -86,8 +84,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64
   }
 }
 
-__device__ __forceinline__ void named_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
-
 // fp32 -> (bf16 high, bf16 low) pairs packed two per 32-bit word
 __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(hi) : "f"(b), "f"(a));
@@ -106,56 +102,80 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
         "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                                                               \
       : "r"(taddr))
 
-__global__ void __launch_bounds__(kThreadsTC, 1)
-dense6_tc_kernel(float2* __restrict__ psi, uint64_t ncols, const uint4* __restrict__ wops, unsigned* err,
-                 uint64_t limit_ns) {
-  extern __shared__ __align__(1024) unsigned char smem_tc[];
-  __shared__ __align__(8) uint64_t s_mbar[kWG];
-  __shared__ uint32_t s_tmem;
-  __shared__ int s_ok[kWG];
-  const int t = threadIdx.x;
-  const int wg = t >> 7, tl = t & 127, warp = (t >> 5) & 3;
-  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem_tc);
-  const uint32_t w_hi = sbase, w_lo = sbase + kOp;
-  const uint32_t x_hi = sbase + 2 * kOp + wg * 2 * kOp, x_lo = x_hi + kOp;
-  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar[wg]);
+// ---- one warpgroup per block; the next tile is staged while this one computes ----
+// Shared memory: W hi/lo (64 KiB) | X hi/lo (64 KiB, reused as the output staging) | input
+// staging (64 KiB).  Staging rows are 512 B (one state column); 16-byte chunk j of row c sits at
+// chunk position j ^ (c & 7), so the per-row accesses of 8 consecutive threads hit distinct banks
+// while the per-column copies of a warp stay contiguous (coalesced global loads and stores).
+constexpr uint32_t kSmemPipe = 2 * kOp + 2 * kOp + 128 * 512;
 
-  // W (prepared on the host in the canonical layout) -> shared memory
-  for (uint32_t i = t; i < 2 * kOp / 16; i += kThreadsTC) reinterpret_cast<uint4*>(smem_tc)[i] = wops[i];
+__device__ __forceinline__ uint32_t stage_off(int row, int chunk) {
+  return (uint32_t)(row * 512 + ((chunk ^ (row & 7)) << 4));
+}
+
+__device__ __forceinline__ void cp_async16_tc(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+__global__ void __launch_bounds__(128, 1)
+dense6_tc_pipe_kernel(float2* __restrict__ psi, uint64_t ncols, const uint4* __restrict__ wops, unsigned* err,
+                      uint64_t limit_ns) {
+  extern __shared__ __align__(1024) unsigned char smem_p[];
+  __shared__ __align__(8) uint64_t s_mb;
+  __shared__ uint32_t s_tm;
+  __shared__ int s_okp;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem_p);
+  const uint32_t w_hi = sbase, w_lo = sbase + kOp, x_hi = sbase + 2 * kOp, x_lo = x_hi + kOp;
+  const uint32_t stg = sbase + 4 * kOp;
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mb);
+  const uint64_t ntiles = ncols / 128;
+  const float4* src4 = reinterpret_cast<const float4*>(psi);
+  float4* dst4 = reinterpret_cast<float4*>(psi);
+
+  for (uint32_t i = t; i < 2 * kOp / 16; i += 128) reinterpret_cast<uint4*>(smem_p)[i] = wops[i];
   if (t == 0) {
-    for (int g = 0; g < kWG; ++g) {
-      const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&s_mbar[g]);
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
-    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0 && wg == 0) {
-    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&s_tmem);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(kTmemCols)
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&s_tm);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(128)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  // stage the first tile: warp w copies columns 32w..32w+31, lane = 16-byte chunk
+  auto stage = [&](uint64_t tile) {
+    for (int k = 0; k < 32; ++k) {
+      const int row = warp * 32 + k;
+      cp_async16_tc(stg + stage_off(row, lane), src4 + (tile * 128 + row) * 32 + lane);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  uint64_t tile = blockIdx.x;
+  if (tile < ntiles) stage(tile);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = s_tmem + (uint32_t)(wg * 128);   // this warpgroup's 128 accumulator columns
-  const uint64_t ntiles = ncols / 128;
+  const uint32_t tmem = s_tm;
   uint32_t phase = 0;
 
-  for (uint64_t tile = (uint64_t)blockIdx.x * kWG + wg; tile < ntiles; tile += (uint64_t)gridDim.x * kWG) {
-    const uint64_t col = tile * 128 + tl;
-    float4* cp = reinterpret_cast<float4*>(psi + col * 64);
-    // ---- operand X: this thread's column, split into BF16 high / low parts ----
+  for (; tile < ntiles; tile += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();  // the tile is staged (all threads' copies); D of the previous tile is read
+    // ---- convert row t of the staging into the split operand ----
+    const unsigned char* sp = smem_p + 4 * kOp;
 #pragma unroll 4
     for (int j = 0; j < 16; ++j) {
-      const float4 v0 = cp[2 * j], v1 = cp[2 * j + 1];
+      const float4 v0 = *reinterpret_cast<const float4*>(sp + stage_off(t, 2 * j));
+      const float4 v1 = *reinterpret_cast<const float4*>(sp + stage_off(t, 2 * j + 1));
       uint4 h, l;
       split2(v0.x, v0.y, h.x, l.x);
       split2(v0.z, v0.w, h.y, l.y);
       split2(v1.x, v1.y, h.z, l.z);
       split2(v1.z, v1.w, h.w, l.w);
-      const uint32_t off = canon(tl, j);
+      const uint32_t off = canon(t, j);
       asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(x_hi + off), "r"(h.x), "r"(h.y), "r"(h.z),
                    "r"(h.w) : "memory");
       asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(x_lo + off), "r"(l.x), "r"(l.y), "r"(l.z),
@@ -163,28 +183,28 @@ dense6_tc_kernel(float2* __restrict__ psi, uint64_t ncols, const uint4* __restri
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    named_sync(1 + wg);
-    if (tl == 0) {
+    __syncthreads();  // operand complete, staging free
+    const uint64_t next = tile + gridDim.x;
+    if (next < ntiles) stage(next);
+    if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        const uint32_t ko = (uint32_t)k * 256u;  // two K-chunks per K=16 step
+        const uint32_t ko = (uint32_t)k * 256u;
         umma(tmem, sdesc(x_hi + ko), sdesc(w_hi + ko), k > 0 ? 1u : 0u);
         umma(tmem, sdesc(x_hi + ko), sdesc(w_lo + ko), 1u);
         umma(tmem, sdesc(x_lo + ko), sdesc(w_hi + ko), 1u);
       }
       umma_commit(mbar);
-    }
-    // one thread waits for the MMAs (bounded); the warpgroup follows its verdict
-    if (tl == 0) {
-      s_ok[wg] = mbar_wait(mbar, phase, limit_ns) ? 1 : 0;
-      if (!s_ok[wg]) atomicExch(err, (unsigned)DERR_BARRIER_TIMEOUT);
+      s_okp = mbar_wait(mbar, phase, limit_ns) ? 1 : 0;
+      if (!s_okp) atomicExch(err, (unsigned)DERR_BARRIER_TIMEOUT);
     }
     phase ^= 1u;
-    named_sync(1 + wg);
-    if (!s_ok[wg]) break;
+    __syncthreads();
+    if (!s_okp) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // ---- accumulator row tl (TMEM lane 32*warp + lane) = the new column ----
+    // ---- accumulator row t -> the X buffer as FP32 output staging (same swizzled rows) ----
+    unsigned char* op = smem_p + 2 * kOp;
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -193,17 +213,23 @@ dense6_tc_kernel(float2* __restrict__ psi, uint64_t ncols, const uint4* __restri
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
       for (int e = 0; e < 8; ++e)
-        cp[8 * q + e] = make_float4(__uint_as_float(r[4 * e]), __uint_as_float(r[4 * e + 1]),
-                                    __uint_as_float(r[4 * e + 2]), __uint_as_float(r[4 * e + 3]));
+        *reinterpret_cast<uint4*>(op + stage_off(t, 8 * q + e)) =
+            make_uint4(r[4 * e], r[4 * e + 1], r[4 * e + 2], r[4 * e + 3]);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    named_sync(1 + wg);
+    __syncthreads();
+    // ---- coalesced stores: warp w writes columns 32w..32w+31, lane = 16-byte chunk ----
+    for (int k = 0; k < 32; ++k) {
+      const int row = warp * 32 + k;
+      dst4[(tile * 128 + row) * 32 + lane] = *reinterpret_cast<const float4*>(op + stage_off(row, lane));
+    }
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0 && wg == 0) {
+  if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
   }
 }
 
@@ -244,18 +270,18 @@ void dense6_prepare_weights(const std::complex<double>* U, uint8_t* out) {
 }
 
 cudaError_t launch_dense6_tc(void* psi, int n, const void* d_weights, unsigned* err, uint64_t limit_ns,
-                             cudaStream_t s) {
-  if (n < 13) return cudaErrorInvalidValue;  // at least one 128-column tile
-  cudaError_t e = cudaFuncSetAttribute(dense6_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTC);
+                                  cudaStream_t s) {
+  if (n < 13) return cudaErrorInvalidValue;
+  cudaError_t e =
+      cudaFuncSetAttribute(dense6_tc_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPipe);
   if (e != cudaSuccess) return e;
   const uint64_t ncols = 1ull << (n - 6);
   const uint64_t tiles = ncols / 128;
   uint64_t grid = (uint64_t)device_sm_count();
-  const uint64_t need = (tiles + kWG - 1) / kWG;
-  if (grid > need) grid = need;
-  dense6_tc_kernel<<<(unsigned)grid, kThreadsTC, kSmemTC, s>>>(reinterpret_cast<float2*>(psi), ncols,
-                                                                 reinterpret_cast<const uint4*>(d_weights), err,
-                                                                 limit_ns);
+  if (grid > tiles) grid = tiles;
+  dense6_tc_pipe_kernel<<<(unsigned)grid, 128, kSmemPipe, s>>>(reinterpret_cast<float2*>(psi), ncols,
+                                                               reinterpret_cast<const uint4*>(d_weights), err,
+                                                               limit_ns);
   return cudaGetLastError();
 }
 
