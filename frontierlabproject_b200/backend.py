@@ -186,6 +186,20 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
     t0 = time.perf_counter()
     sv.synchronize()
     t_sync = time.perf_counter() - t0
+    counts = None
+    t_sample = 0.0
+    if task == "sampling" and shots:
+        # the runner's sampling task (runner.py:25-27, 74); the reference's custom backend
+        # ignores it.  Device sampler; indices mapped from layout positions to circuit qubits.
+        t0 = time.perf_counter()
+        idx = sv.sample(int(shots))
+        order = layout if not logical_order else list(range(num_qubits))
+        logical = np.zeros_like(idx)
+        for pos, q in enumerate(order):
+            logical |= ((idx >> np.uint64(pos)) & np.uint64(1)) << np.uint64(q)
+        vals, cnt = np.unique(logical, return_counts=True)
+        counts = {format(int(v), f"0{num_qubits}b"): int(c) for v, c in zip(vals, cnt)}
+        t_sample = time.perf_counter() - t0
     if out is not None:
         result = sv.copy_to(out)
     else:
@@ -223,5 +237,7 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
         "graph_builds": st["graph_builds"],
         "hbm_bytes_alg": (num_tiles + num_reorders + 1) * sweep_bytes,
         "hbm_bytes_executed": (st["sweeps"] + st["gate_sweeps"]) * sweep_bytes,
+        "t_sample_s": t_sample,
+        "counts": counts,
     }
     return result, metrics

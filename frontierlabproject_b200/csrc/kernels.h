@@ -47,6 +47,12 @@ void dense6_prepare_weights(const std::complex<double>* U, uint8_t* out);
 cudaError_t launch_dense6_tc(void* psi, int n, const void* d_weights, unsigned* err, uint64_t limit_ns,
                              cudaStream_t s);
 
+// measurement sampling (kern_sample.cu): `shots` indices drawn from |psi|^2, ascending, into
+// out (device); scratch: sample_scratch_bytes(n, shots) bytes of device memory
+size_t sample_scratch_bytes(int n, uint64_t shots);
+cudaError_t launch_sample(int dtype, const void* psi, int n, uint64_t shots, uint64_t seed, void* scratch,
+                          uint64_t* out, cudaStream_t s);
+
 int device_sm_count();
 
 // message returned by qs_last_error() on the calling thread (state.cu)

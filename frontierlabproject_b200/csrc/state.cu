@@ -630,6 +630,25 @@ int qs_materialize(qs_state* s) {
   return guard([&] { if (!s) throw InvalidArg{"null state"}; s->materialize(); });
 }
 
+int qs_sample(qs_state* s, unsigned long long shots, unsigned long long seed, unsigned long long* out) {
+  return guard([&] {
+    if (!s || (!out && shots)) throw InvalidArg{"null argument"};
+    if (shots == 0) return;
+    if (shots > (1ull << 31)) throw InvalidArg{"sample: at most 2^31 shots per call"};
+    s->materialize();  // indices are layout (logical) indices
+    void* scratch = nullptr;
+    uint64_t* d_out = nullptr;
+    CK(cudaMallocAsync(&scratch, sample_scratch_bytes(s->n, shots), s->stream));
+    CK(cudaMallocAsync((void**)&d_out, shots * sizeof(uint64_t), s->stream));
+    CK(launch_sample(s->dtype, s->psi, s->n, shots, seed, scratch, d_out, s->stream));
+    CK(cudaMemcpyAsync(out, d_out, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaFreeAsync(scratch, s->stream));
+    CK(cudaFreeAsync(d_out, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->st.launches += 5;
+  });
+}
+
 int qs_dense6_weights(const double* U, void* out) {
   return guard([&] {
     if (!U || !out) throw InvalidArg{"null argument"};

@@ -178,6 +178,23 @@ class _StatevectorBase:
         """Launch queued ops and the data movement to the current layout (asynchronous)."""
         N.call("qs_materialize", self._h)
 
+    def sample(self, shots: int, seed: int = 0) -> np.ndarray:
+        """``shots`` basis indices drawn from |psi|^2 on the device (ascending, uint64; bit p of
+        an index = layout position p).  Same seed and state give the same indices."""
+        shots = int(shots)
+        if shots < 0:
+            raise RuntimeError("shots must be >= 0")
+        out = np.zeros(shots, dtype=np.uint64)
+        N.call("qs_sample", self._h, shots, int(seed) & 0xFFFFFFFFFFFFFFFF, out.ctypes.data if shots else None)
+        return out
+
+    def sample_counts(self, shots: int, seed: int = 0) -> dict:
+        """Counts per outcome bitstring (qubit 0 rightmost, as Aer's ``get_counts``)."""
+        idx = self.sample(shots, seed)
+        vals, cnt = np.unique(idx, return_counts=True)
+        n = self.num_qubits
+        return {format(int(v), f"0{n}b"): int(c) for v, c in zip(vals, cnt)}
+
     def apply_dense(self, U, qubits: Sequence[int] = (0, 1, 2, 3, 4, 5)) -> None:
         """Dense 64x64 unitary on six layout positions in one tensor-core sweep (complex64,
         >= 13 qubits); row/column index sum_j b_{qubits[j]} 2^j.  Other positions are first

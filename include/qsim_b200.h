@@ -126,6 +126,11 @@ QS_API int qs_materialize(qs_state* s);
  * One sweep on the tensor cores (tcgen05 MMAs, operands split into BF16 high and low parts,
  * FP32 accumulation in tensor memory); queued gates run first and the layout is materialised. */
 QS_API int qs_apply_dense6(qs_state* s, const double* U);
+/* Measurement sampling (the runner's "sampling" task, runner.py:25-27, 74; the reference's custom
+ * backend has none): `shots` basis indices (layout order, bit p = position p) drawn from |psi|^2,
+ * returned ascending in out (host, shots entries).  Queued gates run first.  seed selects the
+ * counter-based random stream (same seed, same state -> same indices). */
+QS_API int qs_sample(qs_state* s, unsigned long long shots, unsigned long long seed, unsigned long long* out);
 /* The tensor-core operand qs_apply_dense6 builds from U (host only; 65536 bytes into out):
  * the 128x128 real form W (row 2r+q, column 2s+p: q,p = 0 real / 1 imaginary part) split into
  * BF16 high and low parts, in the canonical K-major layout (8-row x 16-byte core matrices,
