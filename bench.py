@@ -227,6 +227,14 @@ def adjoint_bench(n: int = 24, layers: int = 20, reps: int = 3, seed: int = 0) -
     ref = AdjointEngine(n, f32=False)
     E64, g64 = ref.energy_and_grad(pc, th, a, b)
     rel = float(np.linalg.norm(g - g64) / np.linalg.norm(g64))
+    # the per-gate reverse sweep (one kernel per gate over both states), for comparison
+    pg = AdjointEngine(n, f32=True, method="per_gate")
+    pg.energy_and_grad(pc, th, a, b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pg.energy_and_grad(pc, th, a, b)
+    t_pg = time.perf_counter() - t0
+    del pg
     # parameter shift with the pass executor
     for _ in range(2):
         eng.energy(pc, th, a, b)
@@ -245,6 +253,7 @@ def adjoint_bench(n: int = 24, layers: int = 20, reps: int = 3, seed: int = 0) -
     return {"workload": f"hardware-efficient ansatz n={n} L={layers} ({pc.num_params} parameters, "
                         f"{len(pc.gates)} gates), complex64 states, FP64 accumulation",
             "gradients_per_s": 1.0 / t_adj, "seconds_per_gradient": t_adj, "energy": E,
+            "method": eng.method, "per_gate_gradients_per_s": 1.0 / t_pg,
             "rel_err_vs_fp64_adjoint": rel, "energy_abs_err_vs_fp64": abs(E - E64),
             "param_shift_gradients_per_s": ps_fast, "param_shift_plain_gradients_per_s": ps_plain,
             "speedup_vs_param_shift": (1.0 / t_adj) / ps_fast,

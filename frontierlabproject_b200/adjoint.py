@@ -82,14 +82,24 @@ class ParamCircuit:
 class AdjointEngine:
     """Energy and gradient of ``ParamCircuit`` expectations on one GPU."""
 
-    def __init__(self, num_qubits: int, f32: bool = True, mode: str = "graphed"):
+    def __init__(self, num_qubits: int, f32: bool = True, mode: str = "graphed", method: str = "auto"):
+        """method: "fused" (complex64: the whole gradient in one persistent launch of the
+        batched kernel, planned passes over psi and lam), "per_gate" (one reverse kernel per
+        gate over the two states), "auto" (fused for complex64 with 2..26 qubits)."""
         cls = StatevectorF32 if f32 else Statevector
         self.n = num_qubits
         self.f32 = f32
         self.mode = mode
+        if method not in ("auto", "fused", "per_gate"):
+            raise ValueError(f"unknown method: {method}")
+        if method == "fused" and not f32:
+            raise ValueError("the fused gradient runs complex64 states")
+        self.method = "fused" if (method == "auto" and f32 and 2 <= num_qubits <= 26) else \
+            ("per_gate" if method == "auto" else method)
         self.psi = cls(num_qubits)
         self.lam = cls(num_qubits)
         self._np_dtype = np.complex64 if f32 else np.complex128
+        self._fused = None      # (structure key, BatchedAdjoint)
 
     def set_config(self, **kw) -> None:
         self.psi.set_config(**kw)
@@ -125,6 +135,26 @@ class AdjointEngine:
         return e.value
 
     def energy_and_grad(self, pc: ParamCircuit, theta, a, b) -> Tuple[float, np.ndarray]:
+        if self.method == "fused":
+            return self._fused_energy_and_grad(pc, theta, a, b)
+        return self._per_gate_energy_and_grad(pc, theta, a, b)
+
+    def _fused_energy_and_grad(self, pc: ParamCircuit, theta, a, b) -> Tuple[float, np.ndarray]:
+        from .batch import BatchedAdjoint, BatchShape, Instance
+        if pc.num_qubits != self.n:
+            raise ValueError("circuit size differs from the engine's")
+        inst = Instance(pc, np.asarray(theta, dtype=np.float64), np.asarray(a, dtype=np.float64),
+                        np.asarray(b, dtype=np.float64))
+        key = (tuple((g.name, g.qubits, g.param) for g in pc.gates), pc.num_params)
+        if self._fused is None or self._fused[0] != key:
+            # 12 staged bits: two blocks per SM (measured faster than 13 for one instance)
+            self._fused = (key, BatchedAdjoint([inst], BatchShape(m=12, small_max=12, chunk=1, threads=256)))
+        else:
+            self._fused[1].update([inst])
+        E, G = self._fused[1].energies_and_grads()
+        return float(E[0]), G[0]
+
+    def _per_gate_energy_and_grad(self, pc: ParamCircuit, theta, a, b) -> Tuple[float, np.ndarray]:
         mats = self._forward(pc, theta)
         E = self._expect(a, b)
         ops = np.zeros(len(pc.gates), dtype=ADJ_OP)

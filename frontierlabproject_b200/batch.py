@@ -133,7 +133,10 @@ class BatchedAdjoint:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            N.lib().qs_batch_destroy(h)
+            try:
+                N.lib().qs_batch_destroy(h)
+            except Exception:  # interpreter shutdown: the library may already be unloaded
+                pass
             self._h = None
 
     def update(self, insts: Sequence[Instance]) -> None:

@@ -173,7 +173,10 @@ struct Encoded {
   std::vector<int> grad0;   // per instance
 };
 
-Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg) {
+// plans: optional per-instance cache (structure signature, planned passes)
+using PlanCache = std::vector<std::pair<uint64_t, std::vector<PlannedPass>>>;
+
+Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* plans = nullptr) {
   const int ninst = (int)insts.size();
   std::vector<BatchInst> bi(ninst);
   std::vector<BatchPass> bp;
@@ -227,7 +230,23 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg) {
     pc.m = m;
     pc.r = std::min(5, m);
     pc.k = 3;
-    auto passes = plan_passes(cops, in.n, pc);
+    // plans depend on the gates' staging requirements and commutation (touch masks), not on
+    // matrix values: reuse the cached plan of the same structure (parameter updates)
+    uint64_t sig = 1469598103934665603ull;
+    for (const COp& c : cops) {
+      const uint64_t w[3] = {c.need, c.touch, (uint64_t)c.kind};
+      for (uint64_t v : w) { sig ^= v; sig *= 1099511628211ull; }
+    }
+    std::vector<PlannedPass> passes;
+    if (plans && (size_t)i < plans->size() && (*plans)[i].first == sig) {
+      passes = (*plans)[i].second;
+    } else {
+      passes = plan_passes(cops, in.n, pc);
+      if (plans) {
+        if (plans->size() <= (size_t)i) plans->resize(i + 1);
+        (*plans)[i] = {sig, passes};
+      }
+    }
     for (const PlannedPass& ps : passes) {
       BatchPass p;
       std::memset(&p, 0, sizeof(p));
@@ -474,6 +493,7 @@ struct qs_batch {
   Cfg cfg;
   std::vector<int> n, nparam;
   Encoded enc;
+  PlanCache plans;             // per instance: reused by parameter updates of the same structure
   uint8_t* d_prog = nullptr;
   void* d_arena = nullptr;
   double* d_grads = nullptr;   // nparam_total, then ninst energies
@@ -501,7 +521,7 @@ int qs_batch_create(const qs_batch_instance* insts, int ninst, const qs_batch_co
     std::unique_ptr<qs_batch> b(new qs_batch);
     b->cfg = c;
     for (auto& x : in) { b->n.push_back(x.n); b->nparam.push_back(x.nparam); }
-    b->enc = encode_batch(in, c);
+    b->enc = encode_batch(in, c, &b->plans);
     BCK(cudaMalloc(&b->d_prog, b->enc.bytes.size()));
     BCK(cudaMemcpy(b->d_prog, b->enc.bytes.data(), b->enc.bytes.size(), cudaMemcpyHostToDevice));
     if (b->enc.arena_amps) BCK(cudaMalloc(&b->d_arena, b->enc.arena_amps * sizeof(float2)));
@@ -520,7 +540,7 @@ int qs_batch_set_params(qs_batch* b, const qs_batch_instance* insts, int ninst) 
     auto in = read_instances(insts, ninst);
     for (int i = 0; i < ninst; ++i)
       if (in[i].n != b->n[i] || in[i].nparam != b->nparam[i]) bad("batch: instance shapes differ from the batch's");
-    Encoded e = encode_batch(in, b->cfg);
+    Encoded e = encode_batch(in, b->cfg, &b->plans);
     if (e.arena_amps != b->enc.arena_amps || e.nparam_total != b->enc.nparam_total)
       bad("batch: instance shapes differ from the batch's");
     BCK(cudaDeviceSynchronize());
