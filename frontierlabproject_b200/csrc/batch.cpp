@@ -184,9 +184,101 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* 
   std::vector<double> coef;
   Encoded E;
   E.grad0.resize(ninst);
+  std::vector<BatchPhase> bph;
   // per instance: stage list (kind, pass, items)
   struct Stage { int kind, pass, nitems; };
   std::vector<std::vector<Stage>> stages(ninst);
+
+  // Passes of instance i with m staged bits and kBatchRegBits register bits per phase.  Plans
+  // depend on the gates' staging requirements and commutation (touch masks), not on matrix
+  // values: the cached plan of the same structure is reused (parameter updates).
+  auto plan_instance = [&](const Inst& in, int i, int m, PlanCache* cache) {
+    std::vector<COp> cops;
+    for (const IGate& g : in.gates) {
+      COp c = classify(g.op);
+      c.need = need_of(g);
+      cops.push_back(c);
+    }
+    PlanConfig pc;
+    pc.m = m;
+    pc.r = std::min(kBatchRegBits, m);
+    pc.k = std::min(3, m);
+    uint64_t sig = 1469598103934665603ull ^ (uint64_t)m;
+    for (const COp& c : cops) {
+      const uint64_t w[3] = {c.need, c.touch, (uint64_t)c.kind};
+      for (uint64_t v : w) { sig ^= v; sig *= 1099511628211ull; }
+    }
+    if (cache && (size_t)i < cache->size() && (*cache)[i].first == sig) return (*cache)[i].second;
+    std::vector<PlannedPass> passes = plan_passes(cops, in.n, pc);
+    if (cache) {
+      if (cache->size() <= (size_t)i) cache->resize(i + 1);
+      (*cache)[i] = {sig, passes};
+    }
+    return passes;
+  };
+
+  // Encode one pass: its gates in phase order, and its register phases unless a gate cannot
+  // run in registers there (then the kernel runs the pass gate by gate in shared memory).
+  auto emit_pass = [&](const PlannedPass& ps, const Inst& in) {
+    BatchPass p;
+    std::memset(&p, 0, sizeof(p));
+    p.m = (int)ps.sbits.size();
+    p.gate0 = (int)bg.size();
+    uint64_t S = 0;
+    int8_t loc[kBatchMaxQubits];
+    for (int q = 0; q < kBatchMaxQubits; ++q) loc[q] = -1;
+    for (int j = 0; j < p.m; ++j) {
+      p.sbit[j] = (int8_t)ps.sbits[j];
+      S |= 1ull << ps.sbits[j];
+      loc[ps.sbits[j]] = (int8_t)j;
+    }
+    int gj = 0;
+    for (int q = 0; q < in.n; ++q) if (!(S >> q & 1ull)) p.gbit[gj++] = (int8_t)q;
+    const int nr = std::min(kBatchRegBits, p.m);
+    bool regs = (int)ps.phases.size() <= kBatchMaxPhases && p.m - nr <= kBatchMaxLocal;
+    std::vector<BatchPhase> mine;
+    int count = 0;
+    for (const PlannedPhase& ph : ps.phases) {
+      BatchPhase h;
+      std::memset(&h, 0, sizeof(h));
+      h.nr = (int8_t)nr;
+      if ((int)ph.rbits.size() != nr) regs = false;
+      uint32_t R = 0;
+      for (int j = 0; j < (int)ph.rbits.size() && j < kBatchRegBits; ++j) {
+        h.rbit[j] = (int8_t)ph.rbits[j];
+        R |= 1u << ph.rbits[j];
+      }
+      std::vector<int> tb;
+      for (int j = 0; j < p.m; ++j) if (!(R >> j & 1u)) tb.push_back(j);
+      tb = order_thread_bits(tb, 0);
+      for (size_t j = 0; j < tb.size(); ++j) h.tbit[j] = (int8_t)tb[j];
+      h.gate0 = (int)bg.size();
+      h.ngate = (int)ph.ops.size();
+      auto reg = [&](int q) { return loc[q] >= 0 && (R >> loc[q] & 1u); };
+      for (int oi : ph.ops) {
+        const BatchGate g = encode_gate(in.gates[oi]);
+        // register path: 1q on a register bit; 2q with exactly one register operand (the
+        // other fixed: controlled gates); diagonals anywhere
+        if (g.kind == BG_1Q && !reg(g.q0)) regs = false;
+        if (g.kind == BG_2Q && (reg(g.q0) == reg(g.q1))) regs = false;
+        bg.push_back(g);
+        ++count;
+      }
+      mine.push_back(h);
+    }
+    p.ngate = count;
+    if (ps.phases.empty()) {  // (no phases planned: gates in pass order)
+      for (int oi : ps.ops) bg.push_back(encode_gate(in.gates[oi]));
+      p.ngate = (int)ps.ops.size();
+      regs = false;
+    }
+    if (regs) {
+      p.phase0 = (int)bph.size();
+      p.nphase = (int)mine.size();
+      bph.insert(bph.end(), mine.begin(), mine.end());
+    }
+    bp.push_back(p);
+  };
   size_t arena = 0;
   int grad = 0;
   for (int i = 0; i < ninst; ++i) {
@@ -204,14 +296,20 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* 
     b.pass0 = (int)bp.size();
     b.m = in.n <= cfg.small_max ? in.n : std::min(cfg.m, in.n);
     if (in.n <= cfg.small_max) {
-      BatchPass p;
-      std::memset(&p, 0, sizeof(p));
-      p.m = in.n;
-      p.gate0 = (int)bg.size();
-      p.ngate = (int)in.gates.size();
-      for (int j = 0; j < in.n; ++j) p.sbit[j] = (int8_t)j;
-      for (const IGate& g : in.gates) bg.push_back(encode_gate(g));
-      bp.push_back(p);
+      // all qubits staged: one pass (its register phases planned like any other pass)
+      std::vector<PlannedPass> one = plan_instance(in, i, in.n, plans);
+      if (one.size() == 1 && (int)one[0].sbits.size() == in.n) {
+        emit_pass(one[0], in);
+      } else {
+        BatchPass p;
+        std::memset(&p, 0, sizeof(p));
+        p.m = in.n;
+        p.gate0 = (int)bg.size();
+        p.ngate = (int)in.gates.size();
+        for (int j = 0; j < in.n; ++j) p.sbit[j] = (int8_t)j;
+        for (const IGate& g : in.gates) bg.push_back(encode_gate(g));
+        bp.push_back(p);
+      }
       b.npass = 1;
       b.psi = b.lam = -1;
       stages[i].push_back({BI_SMALL, 0, 1});
@@ -219,47 +317,10 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* 
     }
     const int m = std::min(cfg.m, in.n);
     if (in.n - m > 14) bad("batch: instance of " + std::to_string(in.n) + " qubits needs m >= " + std::to_string(in.n - 14));
-    // plan: gates as classified ops with the batch kernel's staging requirement
-    std::vector<COp> cops;
-    for (const IGate& g : in.gates) {
-      COp c = classify(g.op);
-      c.need = need_of(g);
-      cops.push_back(c);
-    }
-    PlanConfig pc;
-    pc.m = m;
-    pc.r = std::min(5, m);
-    pc.k = 3;
-    // plans depend on the gates' staging requirements and commutation (touch masks), not on
-    // matrix values: reuse the cached plan of the same structure (parameter updates)
-    uint64_t sig = 1469598103934665603ull;
-    for (const COp& c : cops) {
-      const uint64_t w[3] = {c.need, c.touch, (uint64_t)c.kind};
-      for (uint64_t v : w) { sig ^= v; sig *= 1099511628211ull; }
-    }
-    std::vector<PlannedPass> passes;
-    if (plans && (size_t)i < plans->size() && (*plans)[i].first == sig) {
-      passes = (*plans)[i].second;
-    } else {
-      passes = plan_passes(cops, in.n, pc);
-      if (plans) {
-        if (plans->size() <= (size_t)i) plans->resize(i + 1);
-        (*plans)[i] = {sig, passes};
-      }
-    }
+    std::vector<PlannedPass> passes = plan_instance(in, i, m, plans);
     for (const PlannedPass& ps : passes) {
-      BatchPass p;
-      std::memset(&p, 0, sizeof(p));
-      p.m = (int)ps.sbits.size();
-      if (p.m != m || ps.sbits[0] != 0) bad("batch: planner returned an unexpected staged set");
-      p.gate0 = (int)bg.size();
-      p.ngate = (int)ps.ops.size();
-      uint64_t S = 0;
-      for (int j = 0; j < p.m; ++j) { p.sbit[j] = (int8_t)ps.sbits[j]; S |= 1ull << ps.sbits[j]; }
-      int gj = 0;
-      for (int q = 0; q < in.n; ++q) if (!(S >> q & 1ull)) p.gbit[gj++] = (int8_t)q;
-      for (int oi : ps.ops) bg.push_back(encode_gate(in.gates[oi]));
-      bp.push_back(p);
+      if ((int)ps.sbits.size() != m || ps.sbits[0] != 0) bad("batch: planner returned an unexpected staged set");
+      emit_pass(ps, in);
     }
     b.npass = (int)passes.size();
     arena = (arena + 1) & ~size_t(1);  // 16-byte aligned states
@@ -320,7 +381,10 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* 
   h.off_gate = (int)off; off = align(off + bg.size() * sizeof(BatchGate));
   h.off_item = (int)off; off = align(off + items.size() * sizeof(BatchItem));
   h.off_coef = (int)off; off = align(off + coef.size() * sizeof(double));
+  h.nphase = (int)bph.size();
+  h.off_phase = (int)off; off = align(off + bph.size() * sizeof(BatchPhase));
   E.bytes.assign(off, 0);
+  if (!bph.empty()) std::memcpy(E.bytes.data() + h.off_phase, bph.data(), bph.size() * sizeof(BatchPhase));
   std::memcpy(E.bytes.data(), &h, sizeof(h));
   std::memcpy(E.bytes.data() + h.off_inst, bi.data(), bi.size() * sizeof(BatchInst));
   std::memcpy(E.bytes.data() + h.off_pass, bp.data(), bp.size() * sizeof(BatchPass));

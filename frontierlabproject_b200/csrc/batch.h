@@ -43,10 +43,26 @@ struct BatchGate {
   float2 u[16];      // forward matrix (BG_1Q: 4 entries, BG_DIAG2: 4, BG_2Q: 16)
 };
 
+constexpr int kBatchRegBits = 4;     // register bits per thread in a phase (16 amplitudes per state)
+constexpr int kBatchMaxPhases = 16;  // phases per pass run in registers (more: per-gate path)
+
+// A register phase of a pass: each thread holds the 2^nr amplitudes whose local bits rbit vary
+// (per state), the other local bits (tbit, lane bits first) select the thread's slot.  The
+// phase's gates act on register bits or on bits fixed per slot or per group.
+struct BatchPhase {
+  int8_t rbit[kBatchRegBits];
+  int8_t tbit[kBatchMaxLocal];
+  int8_t nr;                // register bits (kBatchRegBits unless the pass is smaller)
+  int8_t pad[3];
+  int32_t gate0, ngate;     // gates (forward order), index into the gate array
+};
+
 struct BatchPass {
   int32_t m;         // staged bits
   int32_t gate0;     // first gate (forward order), index into the gate array
   int32_t ngate;
+  int32_t phase0;    // register phases of the pass (their gates are gate0 .. gate0 + ngate)
+  int32_t nphase;    // 0: the pass runs gate by gate in shared memory
   int8_t sbit[kBatchMaxLocal];      // qubit of local bit j (ascending)
   int8_t gbit[kBatchMaxQubits];     // qubit of group bit j (ascending), n - m of them
   int8_t pad[1];
@@ -77,6 +93,8 @@ struct BatchHeader {
   int32_t m;                // staged bits of arena instances
   int32_t small_max;        // instances with n <= small_max are SMALL
   int32_t mbuf;             // shared buffers hold 2^mbuf amplitudes each (psi, then lam)
+  int32_t nphase;
+  int32_t off_phase;
   int32_t pad;
 };
 

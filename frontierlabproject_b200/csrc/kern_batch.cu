@@ -194,9 +194,11 @@ __device__ void apply_gate(const BatchGate& gref, float2* A, float2* L, int m, u
 
 // lam[x] = d(x) psi[x] + sum_i b_i psi[x ^ 2^i] for x in [x0, x1) (psi read through L2 when
 // kGlobal); returns the thread's part of sum Re(conj(psi) lam)
-template <bool kGlobal>
+// kSwz (shared memory only): the arrays are indexed through swz64 (register-phase layout)
+template <bool kGlobal, bool kSwz = false>
 __device__ __forceinline__ double hamiltonian(const float2* psi, float2* lam, int n, uint64_t x0, uint64_t x1,
                                               const double* a, const double* b) {
+  auto ix = [](uint64_t x) -> uint64_t { return kSwz ? (uint64_t)swz64((uint32_t)x) : x; };
   double e = 0.0;
   for (uint64_t x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
     double d = 0.0;
@@ -204,27 +206,186 @@ __device__ __forceinline__ double hamiltonian(const float2* psi, float2* lam, in
       const int j = i + 1 == n ? 0 : i + 1;
       d += (((x >> i) ^ (x >> j)) & 1ull) ? -a[i] : a[i];
     }
-    const float2 p = kGlobal ? __ldcg(psi + x) : psi[x];
+    const float2 p = kGlobal ? __ldcg(psi + x) : psi[ix(x)];
     double re = d * p.x, im = d * p.y;
     for (int i = 0; i < n; ++i) {
-      const float2 q = kGlobal ? __ldcg(psi + (x ^ (1ull << i))) : psi[x ^ (1ull << i)];
+      const float2 q = kGlobal ? __ldcg(psi + (x ^ (1ull << i))) : psi[ix(x ^ (1ull << i))];
       re += b[i] * q.x;
       im += b[i] * q.y;
     }
     const float2 out = make_float2((float)re, (float)im);
     if (kGlobal) __stcg(lam + x, out);
-    else lam[x] = out;
+    else lam[ix(x)] = out;
     e += (double)p.x * re + (double)p.y * im;
   }
   return e;
 }
 
+// ---- register phases: 16 amplitudes per thread and state, gates in registers ----------------
+constexpr int kRegs = 1 << kBatchRegBits;
+
+// 2x2 on register bit J (pairs i, i | 2^J); kRev: gradient term of generator GEN first
+template <int J, bool kRev, int GEN>
+__device__ __forceinline__ void pairs_reg(float2 m0, float2 m1, float2 m2, float2 m3, float2 (&a)[kRegs],
+                                          float2 (&l)[kRegs], float& acc) {
+#pragma unroll
+  for (int i = 0; i < kRegs; ++i) {
+    if (i & (1 << J)) continue;
+    const int i1 = i | (1 << J);
+    const float2 p0 = a[i], p1 = a[i1];
+    a[i] = cmac(m0, p0, m1, p1);
+    a[i1] = cmac(m2, p0, m3, p1);
+    if (kRev) {
+      const float2 l0 = l[i], l1 = l[i1];
+      if (GEN == 1) acc += im_cvf(l0, p1) + im_cvf(l1, p0);
+      if (GEN == 2) acc += im_cvf(l0, make_float2(p1.y, -p1.x)) + im_cvf(l1, make_float2(-p0.y, p0.x));
+      if (GEN == 3) acc += im_cvf(l0, p0) - im_cvf(l1, p1);
+      l[i] = cmac(m0, l0, m1, l1);
+      l[i1] = cmac(m2, l0, m3, l1);
+    }
+  }
+}
+
+template <int J, bool kRev>
+__device__ __forceinline__ void pairs_reg_g(int gen, float2 m0, float2 m1, float2 m2, float2 m3, float2 (&a)[kRegs],
+                                            float2 (&l)[kRegs], float& acc) {
+  if (!kRev || gen == 0) pairs_reg<J, kRev, 0>(m0, m1, m2, m3, a, l, acc);
+  else if (gen == 1) pairs_reg<J, kRev, 1>(m0, m1, m2, m3, a, l, acc);
+  else if (gen == 2) pairs_reg<J, kRev, 2>(m0, m1, m2, m3, a, l, acc);
+  else pairs_reg<J, kRev, 3>(m0, m1, m2, m3, a, l, acc);
+}
+
+template <bool kRev>
+__device__ __forceinline__ void pairs_reg_j(int j, int gen, float2 m0, float2 m1, float2 m2, float2 m3,
+                                            float2 (&a)[kRegs], float2 (&l)[kRegs], float& acc) {
+  switch (j) {
+    case 0: pairs_reg_g<0, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    case 1: pairs_reg_g<1, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    case 2: pairs_reg_g<2, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    default: pairs_reg_g<3, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+  }
+}
+
+// One gate of a register phase.  reg[q]: register bit of qubit q in this phase (-1: not in
+// registers); fixed bits come from the slot's local base index or the group base.
+template <bool kRev>
+__device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* reg, const int8_t* loc, uint32_t base,
+                                         uint64_t gb, float2 (&a)[kRegs], float2 (&l)[kRegs], double* gout) {
+  float acc = 0.0f;
+  const int kind = gref.kind, q0 = gref.q0, q1 = gref.q1, gen = gref.gen;
+  auto fixedbit = [&](int q) -> int {
+    const int L = loc[q];
+    return L >= 0 ? (int)((base >> L) & 1u) : (int)((gb >> q) & 1ull);
+  };
+  if (kind == BG_1Q) {
+    const float2 u0 = gref.u[0], u1 = gref.u[1], u2 = gref.u[2], u3 = gref.u[3];
+    if (!kRev) pairs_reg_j<false>(reg[q0], 0, u0, u1, u2, u3, a, l, acc);
+    else pairs_reg_j<true>(reg[q0], gen, cconj(u0), cconj(u2), cconj(u1), cconj(u3), a, l, acc);
+  } else if (kind == BG_DIAG1 || kind == BG_DIAG2) {
+    const bool two = kind == BG_DIAG2;
+    float2 d[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const float2 v = (two || e < 2) ? gref.u[two ? e : (e & 1)] : make_float2(0.f, 0.f);
+      d[e] = kRev ? cconj(v) : v;
+    }
+    if (!two) { d[2] = d[0]; d[3] = d[1]; }
+    const int j0 = reg[q0], f0 = j0 >= 0 ? 0 : fixedbit(q0);
+    const int j1 = two ? reg[q1] : -1, f1 = (two && j1 < 0) ? fixedbit(q1) : 0;
+    const bool z = kRev && gen == 3;
+#pragma unroll
+    for (int i = 0; i < kRegs; ++i) {
+      const int b0 = j0 >= 0 ? ((i >> j0) & 1) : f0;
+      const int b1 = j1 >= 0 ? ((i >> j1) & 1) : f1;
+      const float2 dd = b1 ? (b0 ? d[3] : d[2]) : (b0 ? d[1] : d[0]);
+      const float2 p = a[i];
+      a[i] = cmul(dd, p);
+      if (kRev) {
+        if (z) acc += b0 ? -im_cvf(l[i], p) : im_cvf(l[i], p);
+        l[i] = cmul(dd, l[i]);
+      }
+    }
+  } else if (kind == BG_2Q) {
+    // one operand in registers, the other fixed (block-diagonal in it): its 2x2 block
+    auto M = [&](int r, int c) { return kRev ? cconj(gref.u[4 * c + r]) : gref.u[4 * r + c]; };
+    if (reg[q1] >= 0) {
+      const int f = fixedbit(q0);
+      pairs_reg_j<kRev>(reg[q1], 0, M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), a, l, acc);
+    } else {
+      const int f = fixedbit(q1);
+      pairs_reg_j<kRev>(reg[q0], 0, M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f),
+                        M(2 * f + 1, 2 * f + 1), a, l, acc);
+    }
+  }
+  if (kRev && gen) warp_add((double)acc, gout + gref.grad);
+}
+
+// All register phases of a pass on the staged group (kRev: phases and gates in reverse).
+// Shared-memory layout: local index l at A[swz64(l)] (L likewise).
+template <bool kRev>
+__device__ void run_phases(const BatchGate* gates, const BatchPhase* phs, int nph, float2* A, float2* L, int m,
+                           uint64_t gb, const int8_t* loc, int8_t* reg, double* gout) {
+  for (int hh = 0; hh < nph; ++hh) {
+    const BatchPhase& ph = phs[kRev ? nph - 1 - hh : hh];
+    const int nr = ph.nr;
+    if ((int)threadIdx.x < kBatchMaxQubits) {
+      const int q = threadIdx.x;
+      int r = -1;
+      for (int j = 0; j < nr; ++j)
+        if (loc[q] >= 0 && ph.rbit[j] == loc[q]) r = j;
+      reg[q] = (int8_t)r;
+    }
+    __syncthreads();
+    uint32_t RB[kBatchRegBits];
+#pragma unroll
+    for (int j = 0; j < kBatchRegBits; ++j) RB[j] = j < nr ? swz64(1u << ph.rbit[j]) : 0u;
+    const int nt = m - nr;
+    const int nslots = 1 << nt;
+    for (int s0 = 0; s0 < nslots; s0 += blockDim.x) {
+      const int slot = s0 + (int)threadIdx.x;
+      const bool act = slot < nslots;
+      uint32_t base = 0;
+      for (int j = 0; j < nt; ++j)
+        if ((slot >> j) & 1) base |= 1u << ph.tbit[j];
+      const uint32_t sb = swz64(base);
+      float2 a[kRegs], l[kRegs];
+#pragma unroll
+      for (int i = 0; i < kRegs; ++i) {
+        uint32_t o = sb;
+#pragma unroll
+        for (int j = 0; j < kBatchRegBits; ++j) if ((i >> j) & 1) o ^= RB[j];
+        // registers beyond 2^nr (small passes) and inactive slots hold zeros
+        const bool use = act && (i >> nr) == 0;
+        a[i] = use ? A[o] : make_float2(0.f, 0.f);
+        l[i] = (kRev && use) ? L[o] : make_float2(0.f, 0.f);
+      }
+      for (int k = 0; k < ph.ngate; ++k) {
+        const BatchGate& g = gates[kRev ? ph.gate0 + ph.ngate - 1 - k : ph.gate0 + k];
+        gate_reg<kRev>(g, reg, loc, base, gb, a, l, gout);
+      }
+#pragma unroll
+      for (int i = 0; i < kRegs; ++i) {
+        uint32_t o = sb;
+#pragma unroll
+        for (int j = 0; j < kBatchRegBits; ++j) if ((i >> j) & 1) o ^= RB[j];
+        if (act && (i >> nr) == 0) {
+          A[o] = a[i];
+          if (kRev) L[o] = l[i];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int NT>
-__global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ prog, float2* __restrict__ arena,
+__global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __restrict__ prog, float2* __restrict__ arena,
                                                    double* __restrict__ grads, double* __restrict__ energy,
                                                    unsigned* __restrict__ ctl, uint64_t limit_ns) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Block B;
+  __shared__ BatchPhase s_ph[kBatchMaxPhases];   // register phases of the current pass
+  __shared__ int8_t s_reg[kBatchMaxQubits];      // register bit of each qubit in the current phase
   __shared__ uint64_t s_dep[128 + 64];     // local index -> global offset (bits 0-6 | 7-12)
   __shared__ uint64_t s_gdep[128 + 128];   // group index -> global offset (bits 0-6 | 7-13)
   __shared__ double s_coef[2 * kBatchMaxQubits];
@@ -236,6 +397,7 @@ __global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ p
   const BatchGate* gates = reinterpret_cast<const BatchGate*>(prog + hdr->off_gate);
   const BatchItem* items = reinterpret_cast<const BatchItem*>(prog + hdr->off_item);
   const double* coef = reinterpret_cast<const double*>(prog + hdr->off_coef);
+  const BatchPhase* phases_g = reinterpret_cast<const BatchPhase*>(prog + hdr->off_phase);
   float2* A = reinterpret_cast<float2*>(smem_raw);
   float2* L = A + (1u << hdr->mbuf);
   const unsigned t = threadIdx.x;
@@ -278,6 +440,7 @@ __global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ p
         if ((int)t < kBatchMaxQubits) B.loc[t] = -1;
         __syncthreads();
         if ((int)t < m) B.loc[B.ps.sbit[t]] = (int8_t)t;
+        if ((int)t < B.ps.nphase && (int)t < kBatchMaxPhases) s_ph[t] = phases_g[B.ps.phase0 + t];
         for (int e = (int)t; e < 128 + 64; e += NT) {
           const int lvl = e >= 128, v = lvl ? e - 128 : e;
           uint64_t q = 0;
@@ -304,16 +467,26 @@ __global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ p
     const BatchItem& it = B.it;
     double* gout = grads + B.in.grad0;
 
+    const bool regs = it.kind != BI_HAM && B.ps.nphase > 0;
     if (it.kind == BI_SMALL) {
       const int dim = 1 << n;
+      // |0...0>: index 0 is index 0 in the swizzled layout too
       for (int x = (int)t; x < dim; x += NT) A[x] = make_float2(x == 0 ? 1.f : 0.f, 0.f);
       __syncthreads();
       const BatchGate* gs = gates + B.ps.gate0;
-      for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, n, 0, B.loc, nullptr);
-      const double e = hamiltonian<false>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
-      warp_add(e, energy + it.inst);
-      __syncthreads();
-      for (int k = B.ps.ngate - 1; k >= 0; --k) apply_gate<true>(gs[k], A, L, n, 0, B.loc, gout + gs[k].grad);
+      if (regs) {
+        run_phases<false>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, nullptr);
+        const double e = hamiltonian<false, true>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
+        warp_add(e, energy + it.inst);
+        __syncthreads();
+        run_phases<true>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, gout);
+      } else {
+        for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, n, 0, B.loc, nullptr);
+        const double e = hamiltonian<false>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
+        warp_add(e, energy + it.inst);
+        __syncthreads();
+        for (int k = B.ps.ngate - 1; k >= 0; --k) apply_gate<true>(gs[k], A, L, n, 0, B.loc, gout + gs[k].grad);
+      }
     } else if (it.kind == BI_HAM) {
       const float2* psi = arena + B.in.psi;
       float2* lam = arena + B.in.lam;
@@ -330,19 +503,24 @@ __global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ p
       const uint32_t pairs = 1u << (m - 1);
       for (int g = it.first; g < it.first + it.count; ++g) {
         const uint64_t gb = s_gdep[g & 127] | s_gdep[128 + (g >> 7)];
+        // register phases keep the group at A[swz64(l)] (pairs of local bit 0 stay adjacent)
+        auto sidx = [&](uint32_t l) -> uint32_t { return regs ? swz64(l) : l; };
         if (!rev && it.pass == 0) {
           for (uint32_t x = t; x < (1u << m); x += NT) A[x] = make_float2((gb == 0 && x == 0) ? 1.f : 0.f, 0.f);
         } else {
           for (uint32_t v = t; v < pairs; v += NT) {
             const uint32_t l = v << 1;
             const uint64_t off = gb | s_dep[l & 127] | s_dep[128 + (l >> 7)];
-            cp16(A + l, psi + off);
-            if (rev) cp16(L + l, lam + off);
+            cp16(A + sidx(l), psi + off);
+            if (rev) cp16(L + sidx(l), lam + off);
           }
           cp_wait_all();
         }
         __syncthreads();
-        if (!rev) {
+        if (regs) {
+          if (!rev) run_phases<false>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, nullptr);
+          else run_phases<true>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, gout);
+        } else if (!rev) {
           for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, m, gb, B.loc, nullptr);
         } else {
           for (int k = B.ps.ngate - 1; k >= 0; --k) apply_gate<true>(gs[k], A, L, m, gb, B.loc, gout + gs[k].grad);
@@ -350,8 +528,8 @@ __global__ void __launch_bounds__(NT) batch_kernel(const uint8_t* __restrict__ p
         for (uint32_t v = t; v < pairs; v += NT) {
           const uint32_t l = v << 1;
           const uint64_t off = gb | s_dep[l & 127] | s_dep[128 + (l >> 7)];
-          __stcg(reinterpret_cast<float4*>(psi + off), *reinterpret_cast<const float4*>(A + l));
-          if (rev) __stcg(reinterpret_cast<float4*>(lam + off), *reinterpret_cast<const float4*>(L + l));
+          __stcg(reinterpret_cast<float4*>(psi + off), *reinterpret_cast<const float4*>(A + sidx(l)));
+          if (rev) __stcg(reinterpret_cast<float4*>(lam + off), *reinterpret_cast<const float4*>(L + sidx(l)));
         }
         __syncthreads();
       }

@@ -446,7 +446,7 @@ static uint64_t fnv(uint64_t h, const void* p, size_t n) {
 
 // Thread-bit order: the first five (the lane bits) cover as many shared-memory bank
 // classes as possible, given the swizzle of the dtype.
-static std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype) {
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype) {
   auto cls = [&](int j) {
     if (dtype == 0) return j == 0 ? 0 : 1 + (j - 1) % 3;
     return j % 3;

@@ -59,6 +59,10 @@ struct PlannedPass {
 // Split ops (in order) into passes and phases.
 std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const PlanConfig& cfg);
 
+// Order of a phase's thread bits (local bits not in registers): the lowest five (the lane
+// bits) cover as many shared-memory bank classes of the dtype's swizzle as possible.
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype);
+
 // In-place bit permutation as a sequence of gate-free passes.  perm[b] = destination
 // physical bit of the data now at physical bit b.
 std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, const PlanConfig& cfg);
