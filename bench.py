@@ -395,7 +395,9 @@ def main():
     ap.add_argument("--jit", type=int, default=0, help="0 auto, 1 always, -1 never")
     ap.add_argument("--jit-lr", type=int, default=5)
     ap.add_argument("--jit-blocks", type=int, default=2)
+    ap.add_argument("--jit-packed", type=int, default=0, help="FP32x2 arithmetic in the specialised kernels")
     ap.add_argument("--m", type=int, default=13)
+    ap.add_argument("--k", type=int, default=3, help="lowest physical bits always staged")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
@@ -432,7 +434,8 @@ def main():
     b_alg = (len(plan) + R + 1) * sweep
 
     sv = StatevectorF32(n)
-    sv.set_config(m=args.m, jit=args.jit, jit_lr=args.jit_lr, jit_blocks=args.jit_blocks)
+    sv.set_config(m=args.m, k=args.k, jit=args.jit, jit_lr=args.jit_lr, jit_blocks=args.jit_blocks,
+                  jit_packed=args.jit_packed)
     stream = torch.cuda.ExternalStream(sv.stream)
     apply = {"graphed": sv.apply_tile_graphed, "cooperative": sv.apply_tile_cooperative,
              "sequential": sv.apply_tile_dev}[args.mode]

@@ -28,7 +28,7 @@ OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
 
 class QsConfig(ctypes.Structure):
     _fields_ = [("m", c_int), ("k", c_int), ("hill_iters", c_int), ("grid_mult", c_int), ("jit", c_int),
-                ("jit_lr", c_int), ("jit_blocks", c_int)]
+                ("jit_lr", c_int), ("jit_blocks", c_int), ("jit_packed", c_int)]
 
 
 class QsStats(ctypes.Structure):

@@ -110,6 +110,7 @@ uint64_t fnv(uint64_t h, const void* p, size_t n) {
 struct Ent {
   int cls = 0;          // 0 zero, 1 one, 2 minus one, 3 +i, 4 -i, 5 real, 6 imaginary, 7 general
   std::string var;      // coefficient variable for classes 5..7
+  int off = -1;         // its entry of the coefficient table (-1: a per-thread value)
 };
 
 struct Gen {
@@ -136,9 +137,103 @@ struct Gen {
     e.cls = cls_of(coef[2 * off], coef[2 * off + 1]);
     if (e.cls >= 5) {
       e.var = "k" + std::to_string(nvar++);
+      e.off = off;
       o << "const float2 " << e.var << " = " << kref(off) << ";";
     }
     return e;
+  }
+
+  // ---- packed registers (FP32x2 arithmetic on two amplitudes) ----
+  // packed: the phase's registers are R[q] / I[q] (real / imaginary parts of registers 2q and
+  // 2q + 1); gates that do not act on register bit 0 update both lanes with one packed
+  // instruction, gates on bit 0 read and write single lanes (LDA / STA).
+  bool packed = false;
+  std::vector<uint32_t> splats;               // parameter-block splats: entry * 4 + component
+  std::unordered_map<uint32_t, int> splat_idx;
+  int splat_cap = 0;                          // splats that fit the parameter block
+
+  // {v, v} for component comp (0: x, 1: y, 2: -x, 3: -y) of e: a parameter-block entry
+  // (constant bank operand) when e is a table entry and the block has room, else built from
+  // the variable
+  std::string splat(const Ent& e, int comp) {
+    if (e.off >= 0) {
+      const uint32_t key = (uint32_t)e.off * 4u + (uint32_t)comp;
+      auto it = splat_idx.find(key);
+      int j = -1;
+      if (it != splat_idx.end()) {
+        j = it->second;
+      } else if ((int)splats.size() < splat_cap) {
+        j = (int)splats.size();
+        splats.push_back(key);
+        splat_idx[key] = j;
+      }
+      if (j >= 0) return "kp->s[" + std::to_string(j) + "]";
+    }
+    static const char* c[4] = {".x", ".y", ".x", ".y"};
+    const std::string v = std::string(comp >= 2 ? "-" : "") + e.var + c[comp];
+    return "make_float2(" + v + "," + v + ")";
+  }
+
+  // packed sum_c row[c] * x_c: real part (comp 0) or imaginary part (comp 1); xr / xi name
+  // the operands' packed real / imaginary parts.  Unit entries are adds (a negated one a
+  // multiply-add by M1 = {-1, -1}), the others multiply-adds with splatted coefficients.
+  std::string plin(const Ent* row, const std::vector<std::string>& xr, const std::vector<std::string>& xi,
+                   int comp) {
+    struct Term {
+      std::string k;  // splatted coefficient; empty: +-1
+      std::string x;
+      bool neg;
+    };
+    std::vector<Term> ts;
+    for (size_t c = 0; c < xr.size(); ++c) {
+      const Ent& e = row[c];
+      const std::string& R = xr[c];
+      const std::string& I = xi[c];
+      switch (e.cls) {
+        case 0: break;
+        case 1: ts.push_back({"", comp ? I : R, false}); break;
+        case 2: ts.push_back({"", comp ? I : R, true}); break;
+        case 3: ts.push_back(comp ? Term{"", R, false} : Term{"", I, true}); break;   // +i
+        case 4: ts.push_back(comp ? Term{"", R, true} : Term{"", I, false}); break;   // -i
+        case 5: ts.push_back({splat(e, 0), comp ? I : R, false}); break;
+        case 6:
+          if (comp) ts.push_back({splat(e, 1), R, false});
+          else ts.push_back({splat(e, 3), I, false});
+          break;
+        default:
+          if (comp) {
+            ts.push_back({splat(e, 0), I, false});
+            ts.push_back({splat(e, 1), R, false});
+          } else {
+            ts.push_back({splat(e, 0), R, false});
+            ts.push_back({splat(e, 3), I, false});
+          }
+      }
+    }
+    if (ts.empty()) return "make_float2(0.f,0.f)";
+    std::string acc;
+    auto first = std::find_if(ts.begin(), ts.end(), [](const Term& t) { return t.k.empty() && !t.neg; });
+    if (first != ts.end()) {
+      acc = first->x;
+      ts.erase(first);
+    } else {
+      const Term t = ts.front();
+      ts.erase(ts.begin());
+      acc = t.k.empty() ? "__fmul2_rn(" + t.x + ",M1)" : "__fmul2_rn(" + t.k + "," + t.x + ")";
+    }
+    for (const Term& t : ts) {
+      if (t.k.empty())
+        acc = t.neg ? "__ffma2_rn(" + t.x + ",M1," + acc + ")" : "__fadd2_rn(" + acc + "," + t.x + ")";
+      else
+        acc = "__ffma2_rn(" + t.k + "," + t.x + "," + acc + ")";
+    }
+    return acc;
+  }
+
+  // register access in the emitted loops: a[i] (interleaved) or one lane of R / I (packed)
+  std::string rd(const std::string& i) const { return packed ? "LDA(" + i + ")" : "a[" + i + "]"; }
+  std::string wr(const std::string& i, const std::string& v) const {
+    return packed ? "STA(" + i + "," + v + ");" : "a[" + i + "]=" + v + ";";
   }
   static Ent cst(int cls) { Ent e; e.cls = cls; return e; }
   Ent cls_ent(int off) const { return cst(cls_of(coef[2 * off], coef[2 * off + 1])); }
@@ -272,31 +367,74 @@ struct Gen {
   // 2x2 on register bit J
   void pairs(int J, const Ent* m) {
     if (is_identity(m, 2)) return;
+    if (packed && J > 0) { ppairs(J, m, ""); return; }
     static const char* x[2] = {"x0", "x1"};
-    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
-      << (1 << J) << "];a[i]=" << lin(m, x, 2) << ";a[i|" << (1 << J) << "]=" << lin(m + 2, x, 2) << ";}\n";
+    const std::string B = std::to_string(1 << J);
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << B << ")){const float2 x0=" << rd("i") << ",x1="
+      << rd("i|" + B) << ";" << wr("i", lin(m, x, 2)) << wr("i|" + B, lin(m + 2, x, 2)) << "}\n";
   }
   // 2x2 on register bit J, applied where the runtime condition holds (selects, no divergence)
   void pairs_sel(int J, const Ent* m, const std::string& cond) {
     if (is_identity(m, 2)) return;
+    if (packed && J > 0) { ppairs(J, m, cond); return; }
     static const char* x[2] = {"x0", "x1"};
-    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (1 << J) << ")){const float2 x0=a[i],x1=a[i|"
-      << (1 << J) << "];const float2 y0=" << lin(m, x, 2) << ",y1=" << lin(m + 2, x, 2) << ";a[i]=(" << cond
-      << ")?y0:x0;a[i|" << (1 << J) << "]=(" << cond << ")?y1:x1;}\n";
+    const std::string B = std::to_string(1 << J);
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << B << ")){const float2 x0=" << rd("i") << ",x1="
+      << rd("i|" + B) << ";const float2 y0=" << lin(m, x, 2) << ",y1=" << lin(m + 2, x, 2) << ";"
+      << wr("i", "(" + cond + ")?y0:x0") << wr("i|" + B, "(" + cond + ")?y1:x1") << "}\n";
+  }
+  // packed 2x2 on register bit J >= 1 (both lanes at once); cond: applied where it holds
+  void ppairs(int J, const Ent* m, const std::string& cond) {
+    const std::string b = std::to_string(1 << (J - 1));
+    const std::vector<std::string> xr = {"r0", "r1"}, xi = {"i0", "i1"};
+    o << "\n#pragma unroll\nfor(int q=0;q<NQ;++q) if(!(q&" << b << ")){const float2 r0=R[q],i0=I[q],r1=R[q|" << b
+      << "],i1=I[q|" << b << "];";
+    const std::string y0 = plin(m, xr, xi, 0), y1 = plin(m, xr, xi, 1), y2 = plin(m + 2, xr, xi, 0),
+                      y3 = plin(m + 2, xr, xi, 1);
+    if (cond.empty()) {
+      o << "R[q]=" << y0 << ";I[q]=" << y1 << ";R[q|" << b << "]=" << y2 << ";I[q|" << b << "]=" << y3 << ";}\n";
+    } else {
+      o << "const float2 y0=" << y0 << ",y1=" << y1 << ",y2=" << y2 << ",y3=" << y3 << ";const bool c_=(bool)("
+        << cond << ");R[q]=c_?y0:r0;I[q]=c_?y1:i0;R[q|" << b << "]=c_?y2:r1;I[q|" << b << "]=c_?y3:i1;}\n";
+    }
   }
   // 4x4 on register bits (JA = matrix bit 0, JB = matrix bit 1)
   void quads(int JA, int JB, const Ent* m) {
     if (is_identity(m, 4)) return;
+    if (packed && JA > 0 && JB > 0) { pquads(JA, JB, m); return; }
     static const char* x[4] = {"x0", "x1", "x2", "x3"};
-    const int A = 1 << JA, B = 1 << JB;
-    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (A | B) << ")){const float2 x0=a[i],x1=a[i|" << A
-      << "],x2=a[i|" << B << "],x3=a[i|" << (A | B) << "];";
-    o << "a[i]=" << lin(m, x, 4) << ";a[i|" << A << "]=" << lin(m + 4, x, 4) << ";a[i|" << B
-      << "]=" << lin(m + 8, x, 4) << ";a[i|" << (A | B) << "]=" << lin(m + 12, x, 4) << ";}\n";
+    const std::string A = std::to_string(1 << JA), B = std::to_string(1 << JB),
+                      AB = std::to_string((1 << JA) | (1 << JB));
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << AB << ")){const float2 x0=" << rd("i") << ",x1="
+      << rd("i|" + A) << ",x2=" << rd("i|" + B) << ",x3=" << rd("i|" + AB) << ";";
+    o << wr("i", lin(m, x, 4)) << wr("i|" + A, lin(m + 4, x, 4)) << wr("i|" + B, lin(m + 8, x, 4))
+      << wr("i|" + AB, lin(m + 12, x, 4)) << "}\n";
+  }
+  // packed 4x4 on register bits JA, JB >= 1
+  void pquads(int JA, int JB, const Ent* m) {
+    const std::string A = std::to_string(1 << (JA - 1)), B = std::to_string(1 << (JB - 1)),
+                      AB = std::to_string((1 << (JA - 1)) | (1 << (JB - 1)));
+    const std::vector<std::string> xr = {"r0", "r1", "r2", "r3"}, xi = {"i0", "i1", "i2", "i3"};
+    o << "\n#pragma unroll\nfor(int q=0;q<NQ;++q) if(!(q&" << AB << ")){const float2 r0=R[q],i0=I[q],r1=R[q|" << A
+      << "],i1=I[q|" << A << "],r2=R[q|" << B << "],i2=I[q|" << B << "],r3=R[q|" << AB << "],i3=I[q|" << AB << "];";
+    const std::string idx[4] = {"q", "q|" + A, "q|" + B, "q|" + AB};
+    std::string y[8];
+    for (int r = 0; r < 4; ++r) {
+      y[2 * r] = plin(m + 4 * r, xr, xi, 0);
+      y[2 * r + 1] = plin(m + 4 * r, xr, xi, 1);
+    }
+    for (int r = 0; r < 4; ++r) o << "R[" << idx[r] << "]=" << y[2 * r] << ";I[" << idx[r] << "]=" << y[2 * r + 1] << ";";
+    o << "}\n";
   }
   // every amplitude times a (possibly selected) scalar
   void scale(const Ent& d) {
     if (d.cls == 1) return;
+    if (packed) {
+      const std::vector<std::string> xr = {"r0"}, xi = {"i0"};
+      o << "\n#pragma unroll\nfor(int q=0;q<NQ;++q){const float2 r0=R[q],i0=I[q];R[q]=" << plin(&d, xr, xi, 0)
+        << ";I[q]=" << plin(&d, xr, xi, 1) << ";}\n";
+      return;
+    }
     static const char* x[1] = {"x0"};
     o << "\n#pragma unroll\nfor(int i=0;i<NR;++i){const float2 x0=a[i];a[i]=" << lin(&d, x, 1) << ";}\n";
   }
@@ -420,6 +558,11 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
       break;
     }
     case GK_1Q_X: {
+      // packed registers: X on the lane bit only flips the frame (the stores swap the lanes)
+      if (G.packed && g.a == 0) {
+        G.toggle_mask(0, "true");
+        break;
+      }
       // register rename; X commutes with the frame
       Ent m[4] = {Gen::cst(0), Gen::cst(1), Gen::cst(1), Gen::cst(0)};
       G.pairs(g.a, m);
@@ -539,6 +682,8 @@ __device__ __forceinline__ float2 ldk_(const float2* p) {
   return v;
 }
 #define LK(i) ldk_(K + (i))
+#define LDA(i) (((i)&1)?make_float2(R[(i)>>1].y,I[(i)>>1].y):make_float2(R[(i)>>1].x,I[(i)>>1].x))
+#define STA(i,v) do{const float2 t_=(v);if((i)&1){R[(i)>>1].y=t_.x;I[(i)>>1].y=t_.y;}else{R[(i)>>1].x=t_.x;I[(i)>>1].x=t_.y;}}while(0)
 )";
 
 }  // namespace
@@ -562,10 +707,13 @@ uint64_t jit_key(const Program& prog, const JitConfig& cfg) {
   std::vector<uint8_t> cls(hdr->ncoef);
   for (int i = 0; i < hdr->ncoef; ++i) cls[i] = (uint8_t)cls_of(cf[2 * i], cf[2 * i + 1]);
   h = fnv(h, cls.data(), cls.size());
-  return fnv(h, &cfg.blocks, sizeof(cfg.blocks));
+  h = fnv(h, &cfg.blocks, sizeof(cfg.blocks));
+  const int pk = cfg.packed ? 1 : 0;
+  return fnv(h, &pk, sizeof(pk));
 }
 
-std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg) {
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg,
+                       std::vector<std::vector<uint32_t>>* splats_out) {
   const uint8_t* b = prog.bytes.data();
   const ProgramHeader* hdr = (const ProgramHeader*)b;
   if (hdr->dtype != 0) throw std::runtime_error("jit: complex64 programs only");
@@ -579,8 +727,19 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
   for (int p = pass_begin; p < pass_end; ++p) {
     const PassDesc& pd = pds[p];
     pass_coef_range(b, p, &G.kbase, &G.kcount);
-    G.o << "struct KP" << p << "{float2 k[" << std::max(1, G.kcount) << "];};\n";
-    G.o << "struct X" << p << "{const KP" << p << "* kp;\n";
+    // packed registers when every phase holds local bit 0 in register bit 0
+    bool packed = cfg.packed && pd.nphase > 0 && !pd.store_perm;
+    for (int h = 0; h < pd.nphase && packed; ++h)
+      if (phs[pd.phase0 + h].rbit[0] != 0) packed = false;
+    G.packed = packed;
+    G.splats.clear();
+    G.splat_idx.clear();
+    G.splat_cap = packed ? std::max(0, kParamCoefs - std::max(1, G.kcount)) : 0;
+    // the pass's struct X is generated first: its splats size the parameter block
+    std::ostringstream outer;
+    outer.swap(G.o);
+    G.o << "struct X" << p << "{const KP" << p << "* kp;\nstatic constexpr bool kPacked=" << (packed ? "true" : "false")
+        << ";\n";
     // swizzled byte offsets of each phase's register bits: immediates
     G.o << "template<typename Real,int LR>__device__ __forceinline__ void reg_offsets(const qsb::PhaseDesc*,int h,"
         << "uint32_t (&B)[LR])const{switch(h){";
@@ -591,19 +750,26 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       G.o << "break;";
     }
     G.o << "default:break;}}\n";
-    // register bit holding local bit 0 per phase (16-byte pair accesses), -1 if none
-    G.o << "template<int LR>__device__ __forceinline__ int pair_reg(const qsb::PhaseDesc*,int h)const{switch(h){";
-    for (int h = 0; h < pd.nphase; ++h) {
-      const PhaseDesc& ph = phs[pd.phase0 + h];
-      int jr = -1;
-      for (int j = 0; j < pd.r; ++j)
-        if (ph.rbit[j] == 0) jr = j;
-      if (jr >= 0) G.o << "case " << h << ":return " << jr << ";";
+    if (packed) {
+      G.o << "template<int LR>__device__ __forceinline__ uint32_t run_packed(const uint8_t* prog,int h,"
+          << "float2 (&R)[1<<(LR-1)],float2 (&I)[1<<(LR-1)],uint64_t pb)const{constexpr int NR=1<<LR;"
+          << "constexpr int NQ=NR/2;const float2 M1=make_float2(-1.f,-1.f);(void)M1;(void)NR;"
+          << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
+    } else {
+      // register bit holding local bit 0 per phase (16-byte pair accesses), -1 if none
+      G.o << "template<int LR>__device__ __forceinline__ int pair_reg(const qsb::PhaseDesc*,int h)const{switch(h){";
+      for (int h = 0; h < pd.nphase; ++h) {
+        const PhaseDesc& ph = phs[pd.phase0 + h];
+        int jr = -1;
+        for (int j = 0; j < pd.r; ++j)
+          if (ph.rbit[j] == 0) jr = j;
+        if (jr >= 0) G.o << "case " << h << ":return " << jr << ";";
+      }
+      G.o << "default:return -1;}}\n";
+      G.o << "template<typename C,int LR>__device__ __forceinline__ uint32_t run("
+          << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
+          << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     }
-    G.o << "default:return -1;}}\n";
-    G.o << "template<typename C,int LR>__device__ __forceinline__ uint32_t run("
-        << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
-        << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
     for (int h = 0; h < pd.nphase; ++h) {
       const PhaseDesc& ph = phs[pd.phase0 + h];
       G.o << "case " << h << ":{\nfloat2 fa=make_float2(1.f,0.f);\n";
@@ -616,11 +782,15 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         if (fixed_diag(gis[ph.gate0 + gi])) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
       int absorber = -1;
       if (G.used_fa) {
-        double best = 4.0;  // instructions per amplitude of the separate multiply
+        // packed kernels: only gates on register bit 0 (single-lane arithmetic) absorb; the
+        // separate packed multiply costs two instructions per amplitude
+        double best = packed ? 2.0 : 4.0;  // instructions per amplitude of the separate multiply
         for (int gi = 0; gi < ph.ngate; ++gi) {
+          const GateInstr& gg = gis[ph.gate0 + gi];
+          if (packed && gg.a != 0 && (gg.kind < GK_2Q_DENSE || gg.b != 0)) continue;
           Ent m[16];
           int d = 0;
-          if (!absorber_matrix(G, gis[ph.gate0 + gi], m, &d)) continue;
+          if (!absorber_matrix(G, gg, m, &d)) continue;
           const double added = Gen::fold_added(m, d);
           if (added < best) { best = added; absorber = gi; }
         }
@@ -639,16 +809,30 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         if (!G.mask[j].empty()) G.o << "|(" << G.mask[j] << "?" << (1u << ph.rbit[j]) << "u:0u)";
       G.o << ";}\n";
     }
+    G.o << "default:break;}return 0u;}};\n";
+    const std::string xs = G.o.str();
+    G.o.swap(outer);
+    G.o << "struct KP" << p << "{float2 k[" << std::max(1, G.kcount) << "];";
+    if (!G.splats.empty()) G.o << "float2 s[" << G.splats.size() << "];";
+    G.o << "};\n" << xs;
+    if (splats_out) splats_out->push_back(G.splats);
     std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
-    // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block.  The bound
-    // is the block size every pass of the program is launched with (>= this pass's threads).
-    // The pass's coefficients are the by-value parameter kp (constant bank): the arithmetic
-    // reads them as operands, with no load instruction and no register.
-    G.o << "default:break;}return 0u;}};\nextern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ","
-        << cfg.blocks << ") " << kname << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,"
-        << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};"
-        << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
-        << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,nullptr,0ull);}\n";
+    // blocks == 1: double-buffered group loads; blocks == 2: one buffer per block; blocks == 3:
+    // two teams per block over three buffers.  The bound is the block size every pass of the
+    // program is launched with (>= this pass's threads per team).  The pass's coefficients
+    // are the by-value parameter kp (constant bank): the arithmetic reads them as operands,
+    // with no load instruction and no register.
+    const bool teams = cfg.blocks == 3;
+    G.o << "extern \"C\" __global__ void __launch_bounds__("
+        << (teams ? 2 : 1) * hdr->max_threads << "," << (teams ? 1 : cfg.blocks) << ") " << kname
+        << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
+        << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};";
+    if (teams)
+      G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << ">(ex,prog,psi," << p << ",err,"
+          << kDeviceWaitLimitNs << "ull);}\n";
+    else
+      G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
+          << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,err,0ull);}\n";
   }
   return G.o.str();
 }
@@ -664,8 +848,8 @@ bool compile_source(const std::string& src, std::vector<char>* cubin, std::strin
   }
   const std::string inc = "-I" + csrc_dir();
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", inc.c_str(),
-                        "--extra-device-vectorization", "-lineinfo", "--ptxas-options=-v"};
-  const int rc = nv.compile(prog, verbose ? 7 : 6, opts);
+                        "--extra-device-vectorization", "-lineinfo", "--disable-warnings", "--ptxas-options=-v"};
+  const int rc = nv.compile(prog, verbose ? 8 : 7, opts);
   size_t ls = 0;
   nv.log_size(prog, &ls);
   std::string lg(ls, '\0');
@@ -687,15 +871,26 @@ std::list<std::shared_ptr<JitKernels>> g_cache;  // most recent first
 
 }  // namespace
 
-bool jit_compile_check(const Program& prog, std::string* log, const JitConfig& cfg) {
+// Two teams need whole warps per team (named barriers count warps): programs whose team
+// would be smaller than a warp run one buffer per block instead.
+JitConfig jit_effective(const Program& prog, const JitConfig& cfg) {
+  JitConfig e = cfg;
+  const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
+  if (e.blocks == 3 && hdr->max_threads % 32 != 0) e.blocks = 2;
+  return e;
+}
+
+bool jit_compile_check(const Program& prog, std::string* log, const JitConfig& cfg_in) {
   if (!nvrtc().ok) { if (log) *log = nvrtc().why; return false; }
+  const JitConfig cfg = jit_effective(prog, cfg_in);
   const ProgramHeader* hdr = (const ProgramHeader*)prog.bytes.data();
   return compile_source(jit_source(prog, 0, hdr->npass, jit_key(prog, cfg), cfg), nullptr, log, true);
 }
 
-std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
+std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg_in) {
   std::string why;
   if (!jit_available(&why)) throw std::runtime_error("jit: " + why);
+  const JitConfig cfg = jit_effective(prog, cfg_in);
   const uint64_t key = jit_key(prog, cfg);
   {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -713,6 +908,7 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
   unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const int nchunk = std::max(1, std::min<int>(npass, (int)std::min(hw, 32u)));
   std::vector<std::vector<char>> cubins(nchunk);
+  std::vector<std::vector<std::vector<uint32_t>>> splats(nchunk);
   std::vector<std::string> logs(nchunk);
   std::vector<int> ok(nchunk, 0);
   std::vector<std::pair<int, int>> range(nchunk);
@@ -722,7 +918,8 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
     for (int c = 0; c < nchunk; ++c)
       th.emplace_back([&, c] {
         try {
-          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key, cfg), &cubins[c], &logs[c]);
+          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key, cfg, &splats[c]), &cubins[c],
+                                 &logs[c]);
         } catch (const std::exception& e) {
           logs[c] = e.what();
         }
@@ -737,6 +934,9 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
   k->cbase.resize(npass);
   k->ccount.resize(npass);
   for (int p = 0; p < npass; ++p) pass_coef_range(prog.bytes.data(), p, &k->cbase[p], &k->ccount[p]);
+  for (int c = 0; c < nchunk; ++c)
+    for (auto& v : splats[c]) k->splats.push_back(std::move(v));
+  if ((int)k->splats.size() != npass) throw std::runtime_error("jit: parameter layout of a pass missing");
   Driver& d = driver();
   char kname[64];
   for (int c = 0; c < nchunk; ++c) {
@@ -747,7 +947,9 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
       std::snprintf(kname, sizeof(kname), "qp_%016llx_%d", (unsigned long long)key, p);
       CUfunction f;
       if (d.get_fn(&f, mod, kname) != CUDA_SUCCESS) throw std::runtime_error("jit: kernel not found");
-      if (d.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, kMaxDynamicSmem) != CUDA_SUCCESS)
+      // two teams: three complex64 groups of at most 2^13 amplitudes
+      const int dyn = cfg.blocks == 3 ? 3 * (8 << 13) : kMaxDynamicSmem;
+      if (d.set_attr(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn) != CUDA_SUCCESS)
         throw std::runtime_error("jit: cannot raise the shared-memory limit");
       k->functions.push_back(f);
     }
@@ -760,14 +962,31 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg) {
 }
 
 cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
-                       int threads, size_t smem_double, int sms, cudaStream_t stream) {
+                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream) {
   static const float2 kNone = {0.f, 0.f};
   // the driver copies the parameter block (the pass's coefficients) at the launch call
-  const void* kp = k.ccount[p] > 0 ? (const void*)((const float2*)host_coef + k.cbase[p]) : (const void*)&kNone;
-  void* args[] = {(void*)&d_prog, (void*)&psi, const_cast<void*>(kp)};
-  const unsigned smem = (unsigned)(k.blocks == 1 ? smem_double : smem_double / 2);
-  CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)(k.blocks * sms), 1, 1, threads, 1, 1, smem,
-                               (CUstream)stream, args, nullptr);
+  const float2* hc = (const float2*)host_coef;
+  const void* kp = k.ccount[p] > 0 ? (const void*)(hc + k.cbase[p]) : (const void*)&kNone;
+  const std::vector<uint32_t>& sp = k.splats[p];
+  thread_local std::vector<float2> block;
+  if (!sp.empty()) {
+    // coefficient range, then the splats {v, v} of the packed arithmetic
+    const int nk = std::max(1, k.ccount[p]);
+    block.assign((size_t)nk + sp.size(), float2{0.f, 0.f});
+    for (int i = 0; i < k.ccount[p]; ++i) block[i] = hc[k.cbase[p] + i];
+    for (size_t j = 0; j < sp.size(); ++j) {
+      const float2 c = hc[sp[j] >> 2];
+      const unsigned comp = sp[j] & 3u;
+      const float v = comp == 0 ? c.x : comp == 1 ? c.y : comp == 2 ? -c.x : -c.y;
+      block[nk + j] = float2{v, v};
+    }
+    kp = block.data();
+  }
+  void* args[] = {(void*)&d_prog, (void*)&psi, (void*)&err, const_cast<void*>(kp)};
+  const unsigned smem = (unsigned)jit_smem_bytes(k.blocks, smem_double);
+  const bool teams = k.blocks == 3;
+  CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)((teams ? 1 : k.blocks) * sms), 1, 1,
+                               (unsigned)((teams ? 2 : 1) * threads), 1, 1, smem, (CUstream)stream, args, nullptr);
   if (r == CUDA_SUCCESS) return cudaSuccess;
   // launch-time rejections (configuration) are reported as such, not as a kernel failure
   if (r == CUDA_ERROR_INVALID_VALUE || r == CUDA_ERROR_LAUNCH_OUT_OF_RESOURCES) return cudaErrorInvalidConfiguration;

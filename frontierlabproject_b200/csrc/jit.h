@@ -18,16 +18,20 @@
 namespace qsb {
 
 // Geometry of the specialised kernels.  The register bits per thread (lr) are fixed when
-// the program is planned (2^(m - lr) threads per block); blocks = 1 double-buffers the
-// group loads inside a block, blocks = 2 gives each of two resident blocks one buffer.
+// the program is planned (2^(m - lr) threads per team); blocks = 1 double-buffers the
+// group loads inside a block, blocks = 2 gives each of two resident blocks one buffer,
+// blocks = 3 runs one block per SM of two teams over three buffers (pass_body_teams).
 struct JitConfig {
   int blocks = 1;
+  bool packed = true;   // FP32x2 registers for passes whose phases all hold local bit 0
 };
 
 struct JitKernels {
   std::vector<void*> functions;  // CUfunction per pass
   std::vector<void*> modules;    // CUmodule per compiled chunk
   std::vector<int> cbase, ccount;  // per pass: coefficient-table range passed as its parameter
+  std::vector<std::vector<uint32_t>> splats;  // per pass: splatted entries after the range
+                                              // (table entry * 4 + component: x, y, -x, -y)
   uint64_t key = 0;
   int blocks = 1;
   double compile_seconds = 0.0;
@@ -41,7 +45,9 @@ bool jit_available(std::string* why);
 uint64_t jit_key(const Program& prog, const JitConfig& cfg);
 
 // CUDA source of the specialised kernels for passes [pass_begin, pass_end).
-std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg);
+// splats (optional): per pass, the splatted coefficients its parameter block carries.
+std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg,
+                       std::vector<std::vector<uint32_t>>* splats = nullptr);
 
 // Compile (cached) the kernels of every pass of a complex64 program.
 std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
@@ -49,9 +55,15 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
 // Launch the specialised kernel of pass p (one launch per pass, no grid barrier).
 // host_coef = the program's coefficient table in host memory: the pass's range of it is
 // copied into the launch's parameter block.  smem_double = bytes of two group buffers
-// (Program::max_smem).
+// (Program::max_smem); threads = the program's team size; err = device error word (bounded
+// waits of the two-team kernels).
 cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
-                       int threads, size_t smem_double, int sms, cudaStream_t stream);
+                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream);
+
+// Dynamic shared memory of a specialised kernel: group buffers for the geometry.
+inline size_t jit_smem_bytes(int blocks, size_t smem_double) {
+  return blocks == 1 ? smem_double : blocks == 2 ? smem_double / 2 : smem_double / 2 * 3;
+}
 
 // Compile a program's source on the host only (tests; returns the NVRTC log on failure).
 bool jit_compile_check(const Program& prog, std::string* log, const JitConfig& cfg = JitConfig());

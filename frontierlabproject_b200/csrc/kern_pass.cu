@@ -275,6 +275,7 @@ __device__ __forceinline__ void apply_gate(const GateInstr g, C* a, const C* __r
 // generic pass kernel: gate instructions interpreted from the program
 // ------------------------------------------------------------------------------------
 struct InterpExec {
+  static constexpr bool kPacked = false;  // registers hold interleaved complex values
   template <typename Real, int LR>
   __device__ __forceinline__ static void reg_offsets(const PhaseDesc* ph, int, uint32_t (&B8)[LR]) {
 #pragma unroll

@@ -1,15 +1,22 @@
 // Device code of a pass (sweep), shared by the generic pass kernel (kern_pass.cu, nvcc)
 // and the specialised kernels generated at plan time (jit.cpp, NVRTC).
 //
-// Per group (one value of the group bits) a block of 256 threads:
-//   load   16-byte cp.async copies -> swizzled shared memory, double-buffered: the next
-//          group's copies are in flight while the current group is processed;
+// Per group (one value of the group bits) a team of 256 threads:
+//   load   16-byte cp.async copies -> swizzled shared memory;
 //   phases each thread reads its 2^LR amplitudes (the phase's register bits) from shared
 //          memory, the Exec policy applies the phase's gates in registers, writes back;
 //   store  shared memory -> 16-byte coalesced global stores, optionally through a bit
 //          permutation of the local bits (in-place permutation passes).
-// Several passes in one launch (cooperative mode) are separated by a grid barrier whose
-// wait is bounded (error word set, kernel returns).
+// Two schedules:
+//   pass_body        one team per block; either two group buffers (the next group's copies
+//                    are in flight while the current group is processed) or one buffer and
+//                    two resident blocks per SM.  Several passes in one launch (cooperative
+//                    mode) are separated by a grid barrier whose wait is bounded.
+//   pass_body_teams  two teams per block over three group buffers: slot s of the block's
+//                    groups is processed by team s & 1 in buffer s % 3, and the team that
+//                    finishes slot s copies slot s + 3 (the other team's) into the buffer it
+//                    has just freed.  Copies are tracked by one mbarrier per buffer; every
+//                    wait is bounded (error word set, the team returns).
 #pragma once
 #include "qsim.h"
 
@@ -97,17 +104,64 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// ---- mbarriers (shared::cta) tracking cp.async copies ----
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// the barrier's pending count drops by one when all of this thread's earlier cp.async copies
+// have completed (the barrier is initialised with one count per arriving thread)
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// non-blocking: true when the phase of the given parity has completed (acquire)
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for a phase: false (error word set unless another wait already set it) when
+// the limit expired or another part of the grid reported an error.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err, uint64_t limit_ns) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try(bar, parity)) {
+    if (err && *(volatile unsigned*)err != 0u) return false;
+    if (global_ns() - t0 > limit_ns) {
+      if (err) atomicCAS(err, 0u, (unsigned)DERR_LOAD_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void named_barrier(unsigned id, unsigned nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 constexpr int kPassThreads = 256;
 
 // Issue the asynchronous load of the group with physical base `gbase` into the shared buffer
 // `buf` (16-byte copies, swizzled destinations).  Items: c64 -> two amplitudes (local bit 0
-// inside the vector), c128 -> one amplitude.  `tbase` = physical offset of this thread's
-// first item.
+// inside the vector), c128 -> one amplitude.  `tbase` = physical offset of thread t's first
+// item.
 template <typename Real>
 __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const typename V2<Real>::T* psi,
-                                               uint64_t gbase, uint64_t tbase, const uint64_t* pv, int T, int V) {
+                                               uint64_t gbase, uint64_t tbase, const uint64_t* pv, int T, int V,
+                                               unsigned t) {
   constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
-  const unsigned t = threadIdx.x;
   if ((int)t >= T) return;
   const uint32_t lt = (uint32_t)t << kItemBits;
   const uint64_t base = gbase | tbase;
@@ -173,200 +227,363 @@ __device__ __forceinline__ void regs_io(int jr, C (&a)[1 << LR], unsigned char* 
   }
 }
 
+// Packed registers (complex64, register bit 0 = local bit 0): R[q] holds the real parts and
+// I[q] the imaginary parts of registers 2q and 2q + 1, so one packed FP32x2 instruction
+// updates two amplitudes.  Shared memory then holds every 16-byte pair split,
+// {re(2q), re(2q + 1), im(2q), im(2q + 1)}, except the group as copied from global memory
+// (interleaved, read by a pass's first phase).  swap stores the two lanes exchanged (local
+// bit 0 left flipped by the phase).
+template <int LR>
+__device__ __forceinline__ void packed_load(float2 (&R)[1 << (LR - 1)], float2 (&I)[1 << (LR - 1)],
+                                            const unsigned char* sm, uint32_t sb8, const uint32_t (&B8)[LR],
+                                            bool interleaved) {
+#pragma unroll
+  for (int q = 0; q < (1 << (LR - 1)); ++q) {
+    uint32_t s = sb8;
+#pragma unroll
+    for (int j = 1; j < LR; ++j)
+      if ((q >> (j - 1)) & 1) s ^= B8[j];
+    const float4 v = *reinterpret_cast<const float4*>(sm + s);
+    if (interleaved) {
+      R[q] = make_float2(v.x, v.z);
+      I[q] = make_float2(v.y, v.w);
+    } else {
+      R[q] = make_float2(v.x, v.y);
+      I[q] = make_float2(v.z, v.w);
+    }
+  }
+}
+template <int LR>
+__device__ __forceinline__ void packed_store(const float2 (&R)[1 << (LR - 1)], const float2 (&I)[1 << (LR - 1)],
+                                             unsigned char* sm, uint32_t sb8, const uint32_t (&B8)[LR], bool swap) {
+#pragma unroll
+  for (int q = 0; q < (1 << (LR - 1)); ++q) {
+    uint32_t s = sb8;
+#pragma unroll
+    for (int j = 1; j < LR; ++j)
+      if ((q >> (j - 1)) & 1) s ^= B8[j];
+    *reinterpret_cast<float4*>(sm + s) =
+        swap ? make_float4(R[q].y, R[q].x, I[q].y, I[q].x) : make_float4(R[q].x, R[q].y, I[q].x, I[q].y);
+  }
+}
+
+// Index deposits that do not change within a pass, tabulated in shared memory once per pass:
+// group index -> physical base, thread index -> local / physical base per phase, per-thread
+// load base and store-permutation source.
+struct PassShared {
+  uint64_t gtab[5 * 128];        // group index -> physical base (5 levels x 7 bits)
+  uint64_t pt[kPhaseTab * 48];   // per phase: physical thread base, t bits 0-3 | 4-8
+  uint64_t base[512];            // per thread: physical offset of its first item
+  uint64_t pv[16];               // physical offset of load/store item row v
+  uint32_t lt[kPhaseTab * 48];   // per phase: local thread base
+  uint32_t stt[512];             // per thread: store-permutation source of its first item
+  uint32_t sv[16];               // store-permutation source local offset of row v
+  PassDesc pd;
+};
+
+// Fills the tables of pass p (all threads of the block; ends with a block barrier).
+template <typename Real>
+__device__ __forceinline__ void pass_setup(PassShared& sh, const uint8_t* __restrict__ prog, int p) {
+  constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
+  const int t = (int)threadIdx.x, nthr = (int)blockDim.x;
+  const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
+  if (t == 0) sh.pd = reinterpret_cast<const PassDesc*>(prog + hdr->off_pass)[p];
+  __syncthreads();
+  const PassDesc& pd = sh.pd;
+  const int m = pd.m;
+  const int T = 1 << (m - pd.r);                    // active threads of this pass (per team)
+  const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (16)
+  const int nt = m - pd.r;                           // thread-index bits
+  for (int v = t; v < V; v += nthr) {
+    const uint32_t lv = ((uint32_t)v * (uint32_t)T) << kItemBits;
+    uint64_t q = 0;
+    uint32_t s = 0;
+    for (int j = 0; j < m; ++j)
+      if ((lv >> j) & 1u) {
+        q |= 1ull << pd.sbit[j];
+        if (pd.store_perm) s |= 1u << pd.store_src[j];
+      }
+    sh.pv[v] = q;
+    sh.sv[v] = s;
+  }
+  for (int e = t; e < 5 * 128; e += nthr) {
+    const int level = e >> 7, idx = e & 127;
+    uint64_t v = 0;
+    for (int j = 0; j < 7; ++j) {
+      const int gb = 7 * level + j;
+      if (gb < pd.ngbits && ((idx >> j) & 1)) v |= 1ull << pd.gbit[gb];
+    }
+    sh.gtab[e] = v;
+  }
+  const int nph_tab = pd.nphase < kPhaseTab ? pd.nphase : kPhaseTab;
+  for (int e = t; e < nph_tab * 48; e += nthr) {
+    const int h = e / 48, k = e % 48;
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+    const int lo = k < 16 ? 0 : 4, val = k < 16 ? k : k - 16, nb = k < 16 ? 4 : 5;
+    uint32_t lt = 0;
+    uint64_t pt = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int j = lo + b;
+      if (j < nt && ((val >> b) & 1)) {
+        lt |= 1u << ph->tbit[j];
+        pt |= 1ull << pd.sbit[ph->tbit[j]];
+      }
+    }
+    sh.lt[e] = lt;
+    sh.pt[e] = pt;
+  }
+  for (int u = t; u < T; u += nthr) {
+    const uint32_t l = (uint32_t)u << kItemBits;
+    sh.base[u] = phys_of_local(l, pd.sbit, m);
+    uint32_t st = 0;
+    if (pd.store_perm)
+      for (int j = 0; j < m; ++j) if ((l >> j) & 1u) st |= 1u << pd.store_src[j];
+    sh.stt[u] = st;
+  }
+  __syncthreads();
+}
+
 // ex.run(prog, ph, pass, h, a, pb) applies the gates of phase h of pass `pass` to the
 // thread's registers a[] (pb = physical index of the thread's register-0 amplitude) and
 // returns the local bits left flipped in the registers (the write-back lands at the
 // flipped addresses); ex.reg_offsets(ph, h, B8) gives the swizzled byte offset of each
 // register bit of phase h.
-// kDouble: two group buffers per block (the next group's copies overlap this group's
-// phases); otherwise one buffer and two resident blocks per SM overlap each other.
-// Index deposits that do not change within a pass (group index -> physical base, thread
-// index -> local/physical base per phase, per-thread load base) are tabulated in shared
-// memory once per pass.
+//
+// The phases of one group in the buffer at byte `bsel` (buffers start one bit above every
+// swizzled byte offset of a group, so addresses are XOR combinations indexing smem_raw
+// directly).  t: thread index within the team; *gbp: physical base of the group (shared);
+// bar(): the team's barrier, after every phase.
+template <typename Real, int LR, typename Exec, typename Bar>
+__device__ __forceinline__ void group_phases(const Exec& ex, const uint8_t* __restrict__ prog, const PassShared& sh,
+                                             int p, uint32_t bsel, const uint64_t* gbp, unsigned t, const Bar& bar) {
+  using C = typename V2<Real>::T;
+  constexpr int NR = 1 << LR;
+  constexpr bool kC64 = sizeof(Real) == 4;
+  constexpr uint32_t kEsz = sizeof(C);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
+  const PassDesc& pd = sh.pd;
+  const int nt = pd.m - pd.r;
+  const bool active = (int)t < (1 << nt);
+  for (int h = 0; h < pd.nphase; ++h) {
+    if (active) {
+      const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+      uint32_t sb;
+      uint64_t pb = *gbp;
+      if (h < kPhaseTab) {
+        const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
+        sb = swz<Real>(sh.lt[e0] | sh.lt[e1]);
+        pb |= sh.pt[e0] | sh.pt[e1];
+      } else {
+        uint32_t lb = 0;
+        for (int j = 0; j < nt; ++j)
+          if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
+        sb = swz<Real>(lb);
+      }
+      uint32_t sb8 = bsel ^ (sb * kEsz);
+      uint32_t B8[LR];  // byte offset of register bit j (swizzled)
+      ex.template reg_offsets<Real, LR>(ph, h, B8);
+      if constexpr (Exec::kPacked) {
+        float2 R[NR / 2], I[NR / 2];
+        if (h == 0) packed_load<LR>(R, I, smem_raw, sb8, B8, true);
+        else packed_load<LR>(R, I, smem_raw, sb8, B8, false);
+        const uint32_t fl = ex.template run_packed<LR>(prog, h, R, I, pb);
+        sb8 ^= swz<Real>(fl & ~1u) * kEsz;
+        opaque(sb8);
+#pragma unroll
+        for (int j = 0; j < LR; ++j) opaque(B8[j]);
+        if (fl & 1u) packed_store<LR>(R, I, smem_raw, sb8, B8, true);  // warp-uniform
+        else packed_store<LR>(R, I, smem_raw, sb8, B8, false);
+      } else {
+        // register bit holding local bit 0 (complex64): its pairs are 16-byte accesses
+        const int jr = kC64 ? ex.template pair_reg<LR>(ph, h) : -1;
+        C a[NR];
+        regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, false, false);
+        // fl: local bits whose values the phase left flipped in the registers
+        const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
+        // a flipped local bit 0 swaps the halves of each 16-byte pair instead
+        const bool swap_pairs = jr >= 0 && (fl & 1u);
+        sb8 ^= swz<Real>(jr >= 0 ? (fl & ~1u) : fl) * kEsz;
+        opaque(sb8);
+#pragma unroll
+        for (int j = 0; j < LR; ++j) opaque(B8[j]);
+        if (swap_pairs) regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, true);  // warp-uniform
+        else regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, false);
+      }
+    }
+    bar();
+  }
+}
+
+// Coalesced global store of the group in the buffer at byte `bsel` (thread t of the team).
+// kSplit: the buffer holds split 16-byte pairs (packed kernels; no store permutation).
+template <typename Real, bool kSplit = false>
+__device__ __forceinline__ void group_store(const PassShared& sh, typename V2<Real>::T* __restrict__ psi,
+                                            uint32_t bsel, uint64_t gb, unsigned t) {
+  using C = typename V2<Real>::T;
+  constexpr bool kC64 = sizeof(Real) == 4;
+  constexpr int kItemBits = kC64 ? 1 : 0;
+  constexpr uint32_t kEsz = sizeof(C);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto at = [&](uint32_t byte) -> const C& { return *reinterpret_cast<const C*>(smem_raw + byte); };
+  const PassDesc& pd = sh.pd;
+  const int m = pd.m;
+  const int T = 1 << (m - pd.r);
+  const int V = 1 << (m - kItemBits) >> (m - pd.r);
+  if ((int)t >= T) return;
+  const uint32_t lt = (uint32_t)t << kItemBits;
+  const uint64_t base = gb | sh.base[t];
+  const uint32_t stt = sh.stt[t];
+  if constexpr (kC64) {
+#pragma unroll
+    for (int v = 0; v < 16; ++v) {
+      if (v >= V) break;
+      float4 val;
+      if (pd.store_perm) {
+        const uint32_t s0 = stt | sh.sv[v];
+        const uint32_t s1 = s0 ^ (1u << pd.store_src[0]);
+        const C x0 = at(bsel ^ (swz<Real>(s0) * kEsz)), x1 = at(bsel ^ (swz<Real>(s1) * kEsz));
+        val = make_float4(x0.x, x0.y, x1.x, x1.y);
+      } else {
+        const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << 1);
+        val = *reinterpret_cast<const float4*>(smem_raw + (bsel ^ (swz<Real>(l) * kEsz)));
+        if (kSplit) val = make_float4(val.x, val.z, val.y, val.w);
+      }
+      __stcg(reinterpret_cast<float4*>(psi + (base | sh.pv[v])), val);
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < 16; ++v) {
+      if (v >= V) break;
+      const uint32_t l = lt | ((uint32_t)v * (uint32_t)T);
+      const uint32_t src = pd.store_perm ? (stt | sh.sv[v]) : l;
+      __stcg(psi + (base | sh.pv[v]), at(bsel ^ (swz<Real>(src) * kEsz)));
+    }
+  }
+}
+
+// One team per block.  kDouble: two group buffers per block (the next group's copies overlap
+// this group's phases); otherwise one buffer and two resident blocks per SM overlap each
+// other.
 template <typename Real, int LR, typename Exec, bool kDouble = true>
 __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restrict__ prog,
                                           typename V2<Real>::T* __restrict__ psi,
                                           int pass_begin, int pass_end, unsigned* bar, unsigned* err,
                                           uint64_t barrier_limit_ns) {
   using C = typename V2<Real>::T;
-  constexpr int NR = 1 << LR;
-  constexpr bool kC64 = sizeof(Real) == 4;
-  constexpr int kItemBits = kC64 ? 1 : 0;
+  constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
+  constexpr uint32_t kEsz = sizeof(C);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ PassDesc pd;
-  __shared__ uint64_t pv[16];                  // physical offset of load/store item row v
-  __shared__ uint32_t sv[16];                  // store-permutation source local offset of row v
-  __shared__ uint64_t s_gtab[5 * 128];         // group index -> physical base (5 levels x 7 bits)
-  __shared__ uint64_t s_pt[kPhaseTab * 48];    // per phase: physical thread base, t bits 0-3 | 4-8
-  __shared__ uint32_t s_lt[kPhaseTab * 48];    // per phase: local thread base
-  __shared__ uint64_t s_base[512];             // per thread: physical offset of its first item
-  __shared__ uint32_t s_stt[512];              // per thread: store-permutation source of its first item
+  __shared__ PassShared sh;
   __shared__ uint64_t s_gb[2];                 // physical base of the current group
-
   const unsigned t = threadIdx.x;
-  const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
+  auto block_bar = [] { __syncthreads(); };
 
   for (int p = pass_begin; p < pass_end; ++p) {
     if (p > pass_begin) {
       if (!grid_barrier(bar, err, barrier_limit_ns)) return;
     }
-    if (t == 0) pd = reinterpret_cast<const PassDesc*>(prog + hdr->off_pass)[p];
-    __syncthreads();
-    const int m = pd.m;
-    const int T = 1 << (m - pd.r);                    // active threads of this pass
-    const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (16)
-    const int nt = m - pd.r;                           // thread-index bits
-    for (int v = (int)t; v < V; v += (int)blockDim.x) {
-      const uint32_t lv = ((uint32_t)v * (uint32_t)T) << kItemBits;
-      uint64_t q = 0;
-      uint32_t s = 0;
-      for (int j = 0; j < m; ++j)
-        if ((lv >> j) & 1u) {
-          q |= 1ull << pd.sbit[j];
-          if (pd.store_perm) s |= 1u << pd.store_src[j];
-        }
-      pv[v] = q;
-      sv[v] = s;
-    }
-    for (int e = (int)t; e < 5 * 128; e += (int)blockDim.x) {
-      const int level = e >> 7, idx = e & 127;
-      uint64_t v = 0;
-      for (int j = 0; j < 7; ++j) {
-        const int gb = 7 * level + j;
-        if (gb < pd.ngbits && ((idx >> j) & 1)) v |= 1ull << pd.gbit[gb];
-      }
-      s_gtab[e] = v;
-    }
-    const int nph_tab = pd.nphase < kPhaseTab ? pd.nphase : kPhaseTab;
-    for (int e = (int)t; e < nph_tab * 48; e += (int)blockDim.x) {
-      const int h = e / 48, k = e % 48;
-      const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
-      const int lo = k < 16 ? 0 : 4, val = k < 16 ? k : k - 16, nb = k < 16 ? 4 : 5;
-      uint32_t lt = 0;
-      uint64_t pt = 0;
-      for (int b = 0; b < nb; ++b) {
-        const int j = lo + b;
-        if (j < nt && ((val >> b) & 1)) {
-          lt |= 1u << ph->tbit[j];
-          pt |= 1ull << pd.sbit[ph->tbit[j]];
-        }
-      }
-      s_lt[e] = lt;
-      s_pt[e] = pt;
-    }
-    for (int u = (int)t; u < T; u += (int)blockDim.x) {
-      const uint32_t l = (uint32_t)u << kItemBits;
-      s_base[u] = phys_of_local(l, pd.sbit, m);
-      uint32_t st = 0;
-      if (pd.store_perm)
-        for (int j = 0; j < m; ++j) if ((l >> j) & 1u) st |= 1u << pd.store_src[j];
-      s_stt[u] = st;
-    }
-    __syncthreads();
-    const uint64_t ngroups = 1ull << pd.ngbits;
-    const bool active = (int)t < T;
-    const uint64_t tbase = active ? s_base[t] : 0ull;
-    // Group buffers: buffer 1 starts at byte (esz << m) of the dynamic shared memory, one bit
-    // above every byte offset of a swizzled local index, so a buffer's addresses are XOR
-    // combinations of byte offsets.  Accesses index smem_raw directly (shared-memory
-    // loads/stores with the array base as the immediate offset).
-    constexpr uint32_t kEsz = sizeof(C);
+    pass_setup<Real>(sh, prog, p);
+    const int m = sh.pd.m;
+    const int T = 1 << (m - sh.pd.r);
+    const int V = 1 << (m - kItemBits) >> (m - sh.pd.r);
+    const uint64_t ngroups = 1ull << sh.pd.ngbits;
+    const uint64_t tbase = (int)t < T ? sh.base[t] : 0ull;
     const uint32_t buf1 = kDouble ? (kEsz << m) : 0u;
-    auto at = [&](uint32_t byte) -> C& { return *reinterpret_cast<C*>(smem_raw + byte); };
 
     uint64_t g = blockIdx.x;
     if (kDouble) {
       if (g < ngroups)
-        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, s_gtab), tbase, pv, T, V);
+        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, sh.gtab), tbase, sh.pv, T, V, t);
       cp_async_commit();
     }
     for (int it = 0; g < ngroups; g += gridDim.x, ++it) {
       const uint32_t bsel = (it & 1) ? buf1 : 0u;  // byte offset of this group's buffer
-      if (t == 0) s_gb[it & 1] = gbase_of(g, s_gtab);  // read after the barrier below
+      if (t == 0) s_gb[it & 1] = gbase_of(g, sh.gtab);  // read after the barrier below
       if (kDouble) {
         const uint64_t gn = g + gridDim.x;
         if (gn < ngroups)
-          prefetch_group<Real>(reinterpret_cast<C*>(smem_raw + (bsel ^ buf1)), psi, gbase_of(gn, s_gtab), tbase, pv,
-                               T, V);
+          prefetch_group<Real>(reinterpret_cast<C*>(smem_raw + (bsel ^ buf1)), psi, gbase_of(gn, sh.gtab), tbase,
+                               sh.pv, T, V, t);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
-        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, s_gtab), tbase, pv, T, V);
+        prefetch_group<Real>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(g, sh.gtab), tbase, sh.pv, T, V, t);
         cp_async_commit();
         cp_async_wait<0>();
       }
       __syncthreads();
-      // ---- phases ----
-      for (int h = 0; h < pd.nphase; ++h) {
-        if (active) {
-          const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
-          uint32_t sb;
-          uint64_t pb = s_gb[it & 1];
-          if (h < kPhaseTab) {
-            const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
-            sb = swz<Real>(s_lt[e0] | s_lt[e1]);
-            pb |= s_pt[e0] | s_pt[e1];
-          } else {
-            uint32_t lb = 0;
-            for (int j = 0; j < nt; ++j)
-              if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
-            sb = swz<Real>(lb);
-          }
-          uint32_t sb8 = bsel ^ (sb * kEsz);
-          uint32_t B8[LR];  // byte offset of register bit j (swizzled)
-          ex.template reg_offsets<Real, LR>(ph, h, B8);
-          // register bit holding local bit 0 (complex64): its pairs are 16-byte accesses
-          const int jr = kC64 ? ex.template pair_reg<LR>(ph, h) : -1;
-          C a[NR];
-          regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, false, false);
-          // fl: local bits whose values the phase left flipped in the registers
-          const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
-          // a flipped local bit 0 swaps the halves of each 16-byte pair instead
-          const bool swap_pairs = jr >= 0 && (fl & 1u);
-          sb8 ^= swz<Real>(jr >= 0 ? (fl & ~1u) : fl) * kEsz;
-          opaque(sb8);
-#pragma unroll
-          for (int j = 0; j < LR; ++j) opaque(B8[j]);
-          if (swap_pairs) regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, true);  // warp-uniform
-          else regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, false);
-        }
-        __syncthreads();
-      }
-      // ---- store ----
-      if (active) {
-        const uint32_t lt = (uint32_t)t << kItemBits;
-        const uint64_t base = s_gb[it & 1] | s_base[t];
-        const uint32_t stt = s_stt[t];
-        if constexpr (kC64) {
-#pragma unroll
-          for (int v = 0; v < 16; ++v) {
-            if (v >= V) break;
-            float4 val;
-            if (pd.store_perm) {
-              const uint32_t s0 = stt | sv[v];
-              const uint32_t s1 = s0 ^ (1u << pd.store_src[0]);
-              const C x0 = at(bsel ^ (swz<Real>(s0) * kEsz)), x1 = at(bsel ^ (swz<Real>(s1) * kEsz));
-              val = make_float4(x0.x, x0.y, x1.x, x1.y);
-            } else {
-              const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << 1);
-              val = *reinterpret_cast<const float4*>(smem_raw + (bsel ^ (swz<Real>(l) * kEsz)));
-            }
-            __stcg(reinterpret_cast<float4*>(psi + (base | pv[v])), val);
-          }
-        } else {
-#pragma unroll
-          for (int v = 0; v < 16; ++v) {
-            if (v >= V) break;
-            const uint32_t l = lt | ((uint32_t)v * (uint32_t)T);
-            const uint32_t src = pd.store_perm ? (stt | sv[v]) : l;
-            __stcg(psi + (base | pv[v]), at(bsel ^ (swz<Real>(src) * kEsz)));
-          }
-        }
-      }
+      group_phases<Real, LR>(ex, prog, sh, p, bsel, &s_gb[it & 1], t, block_bar);
+      group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[it & 1], t);
       __syncthreads();
     }
     cp_async_wait<0>();
     __syncthreads();
+  }
+}
+
+// Two teams of blockDim.x / 2 threads per block, three group buffers of 2^m amplitudes
+// (complex64: 3 x 64 KiB).  One pass per launch.  The block's groups are its slots
+// s = 0, 1, 2, ... (group blockIdx.x + s * gridDim.x): team s & 1 processes slot s in buffer
+// s % 3; after finishing slot s a team copies slot s + 3 into buffer s % 3 for the other team.
+// Team 0 then waits at slot 2k for team 1's slot 2k - 3, team 1 at slot 2k + 1 for team 0's
+// slot 2k - 2: the teams alternate, and each group's copies run while both teams compute.
+template <typename Real, int LR, typename Exec>
+__device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* __restrict__ prog,
+                                                typename V2<Real>::T* __restrict__ psi, int p, unsigned* err,
+                                                uint64_t limit_ns) {
+  using C = typename V2<Real>::T;
+  constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
+  constexpr uint32_t kEsz = sizeof(C);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassShared sh;
+  __shared__ uint64_t s_mbar[3];   // copies into buffer b complete
+  __shared__ uint64_t s_gb[2];     // physical base of each team's current group
+  __shared__ int s_ok[2];          // the team's leader saw its copies complete
+  const unsigned tid = threadIdx.x, TS = blockDim.x >> 1;
+  const unsigned team = tid >= TS ? 1u : 0u, t = tid - team * TS;
+  if (tid == 0)
+    for (int b = 0; b < 3; ++b) mbar_init(&s_mbar[b], TS);
+  pass_setup<Real>(sh, prog, p);  // block barrier: the barriers are initialised
+  const int m = sh.pd.m;
+  const int T = 1 << (m - sh.pd.r);
+  const int V = 1 << (m - kItemBits) >> (m - sh.pd.r);
+  const uint64_t ngroups = 1ull << sh.pd.ngbits;
+  const uint32_t bufb = kEsz << m;
+  const uint64_t tbase = (int)t < T ? sh.base[t] : 0ull;
+  auto group_of = [&](uint64_t s) { return (uint64_t)blockIdx.x + s * (uint64_t)gridDim.x; };
+  // every thread of the loading team arrives once per load (inactive threads immediately)
+  auto load_slot = [&](uint64_t s) {
+    const uint32_t b = (uint32_t)(s % 3u);
+    prefetch_group<Real>(reinterpret_cast<C*>(smem_raw + b * bufb), psi, gbase_of(group_of(s), sh.gtab), tbase,
+                         sh.pv, T, V, t);
+    cp_async_mbar_arrive(&s_mbar[b]);
+  };
+  auto team_bar = [team, TS] { named_barrier(1u + team, TS); };
+  if (team == 0) {
+    if (group_of(0) < ngroups) load_slot(0);
+    if (group_of(2) < ngroups) load_slot(2);
+  } else if (group_of(1) < ngroups) {
+    load_slot(1);
+  }
+  for (uint64_t s = team; group_of(s) < ngroups; s += 2) {
+    const uint32_t b = (uint32_t)(s % 3u);
+    const unsigned parity = (unsigned)((s / 3u) & 1u);
+    if (t == 0) {
+      s_ok[team] = mbar_wait_bounded(&s_mbar[b], parity, err, limit_ns) ? 1 : 0;
+      s_gb[team] = gbase_of(group_of(s), sh.gtab);
+    }
+    team_bar();
+    if (!s_ok[team]) {  // team-uniform: leave with no copy of this thread in flight
+      cp_async_wait<0>();
+      return;
+    }
+    (void)mbar_test(&s_mbar[b], parity);  // completed: acquires the copies for this thread
+    const uint32_t bsel = b * bufb;
+    group_phases<Real, LR>(ex, prog, sh, p, bsel, &s_gb[team], t, team_bar);
+    group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[team], t);
+    team_bar();  // buffer b is free
+    if (group_of(s + 3) < ngroups) load_slot(s + 3);
   }
 }
 

@@ -289,7 +289,7 @@ std::vector<int> bits_of(uint64_t m) {
 }  // namespace
 
 static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const std::vector<int>& pass_ops,
-                                             const std::vector<int>& sbits, int r, int iters) {
+                                             const std::vector<int>& sbits, int r, int iters, bool pair_bit) {
   // Phases choose register bits among the staged physical bits; op need masks are
   // physical, so the phase set is a physical mask, converted to local bits at the end.
   uint64_t Smask = 0;
@@ -299,7 +299,8 @@ static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const 
   std::vector<PlannedPhase> phases;
   std::vector<int> rem = pass_ops, taken, rest;
   while (!rem.empty()) {
-    uint64_t R = choose_set(sc, rem, Smask, 0, rr, iters);
+    const uint64_t forced = (pair_bit && (Smask & 1ull)) ? 1ull : 0ull;
+    uint64_t R = choose_set(sc, rem, Smask, forced, rr, iters);
     sc.run(rem, R, taken);
     if (taken.empty()) throw std::runtime_error("planner: phase made no progress");
     PlannedPhase ph;
@@ -337,7 +338,7 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
     PlannedPass ps;
     ps.sbits = bits_of(S);
     ps.ops = taken;
-    ps.phases = plan_phases(ops, taken, ps.sbits, cfg.r, cfg.hill_iters);
+    ps.phases = plan_phases(ops, taken, ps.sbits, cfg.r, cfg.hill_iters, cfg.pair_bit);
     out.push_back(std::move(ps));
     rest.clear();
     size_t t = 0;
@@ -446,12 +447,17 @@ static uint64_t fnv(uint64_t h, const void* p, size_t n) {
 
 // Thread-bit order: the first five (the lane bits) cover as many shared-memory bank
 // classes as possible, given the swizzle of the dtype.
-std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype) {
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid) {
   auto cls = [&](int j) {
     if (dtype == 0) return j == 0 ? 0 : 1 + (j - 1) % 3;
     return j % 3;
   };
-  std::vector<int> rest = tb, out;
+  // candidates in preference order: bits outside `avoid` first
+  std::vector<int> rest;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int j : tb)
+      if (((avoid >> j) & 1ull) == (uint64_t)pass) rest.push_back(j);
+  std::vector<int> out;
   std::vector<bool> covered(4, false);
   for (int c = 0; c < 4 && out.size() < 5; ++c) {
     for (size_t i = 0; i < rest.size(); ++i) {
@@ -508,7 +514,16 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
       uint64_t Rl = 0;
       for (int j = 0; j < r; ++j) { h.rbit[j] = (int8_t)ph.rbits[j]; Rl |= bit(ph.rbits[j]); }
       for (int j = 0; j < d.m; ++j) if (!(Rl & bit(j))) tb.push_back(j);
-      tb = order_thread_bits(tb, dtype);
+      // controls of controlled gates held by a thread bit: off the lane bits where the bank
+      // classes allow (a warp-uniform control costs no per-amplitude select)
+      uint64_t avoid = 0;
+      for (int oi : ph.ops) {
+        const COp& o = ops[oi];
+        if (o.kind != GK_2Q_CX && o.kind != GK_2Q_CU) continue;
+        for (int j = 0; j < d.m; ++j)
+          if (ps.sbits[j] == o.a && !(Rl & bit(j))) avoid |= bit(j);
+      }
+      tb = order_thread_bits(tb, dtype, avoid);
       for (size_t j = 0; j < tb.size(); ++j) h.tbit[j] = (int8_t)tb[j];
       h.gate0 = (int)gi.size();
       h.ngate = (int)ph.ops.size();

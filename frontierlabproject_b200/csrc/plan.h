@@ -42,6 +42,7 @@ struct PlanConfig {
   int r = 5;              // register bits per thread
   int k = 3;              // lowest physical bits always staged (contiguous runs of 2^k amplitudes)
   int hill_iters = 4;     // hill-climbing rounds when choosing the staged / register sets
+  bool pair_bit = false;  // physical bit 0 is a register bit of every phase (packed kernels)
 };
 
 struct PlannedPhase {
@@ -60,8 +61,9 @@ struct PlannedPass {
 std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const PlanConfig& cfg);
 
 // Order of a phase's thread bits (local bits not in registers): the lowest five (the lane
-// bits) cover as many shared-memory bank classes of the dtype's swizzle as possible.
-std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype);
+// bits) cover as many shared-memory bank classes of the dtype's swizzle as possible, taking
+// bits outside `avoid` (a mask of local bits) first.
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid = 0);
 
 // In-place bit permutation as a sequence of gate-free passes.  perm[b] = destination
 // physical bit of the data now at physical bit b.

@@ -36,6 +36,8 @@ constexpr int kFixed = 64;         // operand >= kFixed: physical bit (operand -
 // dynamic shared-memory limit requested for the pass kernels (two 64 KiB group buffers);
 // static tables take about 30 KiB more, within the 227 KiB per block
 constexpr int kMaxDynamicSmem = 160 * 1024;
+// limit of every bounded device-side wait (grid barriers, group copies of the two-team kernels)
+constexpr unsigned long long kDeviceWaitLimitNs = 20ull * 1000ull * 1000ull * 1000ull;  // 20 s
 
 enum GateKind : uint8_t {
   GK_NONE = 0,
@@ -96,6 +98,7 @@ enum DeviceError : uint32_t {
   DERR_NONE = 0,
   DERR_BARRIER_TIMEOUT = 1,
   DERR_BAD_PROGRAM = 2,
+  DERR_LOAD_TIMEOUT = 3,   // a team's wait for its group copies expired (pass kernel, two teams)
 };
 
 // Bank-spreading swizzle of a local amplitude index inside the shared-memory group.

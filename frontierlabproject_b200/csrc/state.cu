@@ -51,7 +51,7 @@ struct InvalidArg {
   std::string msg;
 };
 
-constexpr uint64_t kBarrierLimitNs = 20ull * 1000ull * 1000ull * 1000ull;  // 20 s
+constexpr uint64_t kBarrierLimitNs = kDeviceWaitLimitNs;
 
 int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
 
@@ -108,6 +108,7 @@ struct qs_state {
   int grid_mult = 0;
   int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
   int jit_lr = 5;          // register bits per thread of the specialised kernels
+  int jit_packed = 0;      // FP32x2 arithmetic in the specialised kernels
   int jit_blocks = 2;      // resident blocks per SM of the specialised kernels (single-buffered
                            // blocks that overlap each other's group loads)
   // device scratch: program buffer, control words (barrier x2, error), accumulators
@@ -212,6 +213,7 @@ struct qs_state {
       if (use_jit) {
         JitConfig jc;
         jc.blocks = jit_blocks;
+        jc.packed = jit_packed != 0;
         jk = jit_get(prog, jc);
         st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
         jk->compile_seconds = 0.0;  // counted once
@@ -228,8 +230,8 @@ struct qs_state {
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int p = 0; p < prog.npass && e == cudaSuccess; ++p)
-          e = jk ? jit_launch(*jk, p, d_prog, host_coef, psi, prog.threads, prog.max_smem, device_sm_count(),
-                              stream)
+          e = jk ? jit_launch(*jk, p, d_prog, host_coef, psi, d_ctl + 2, prog.threads, prog.max_smem,
+                              device_sm_count(), stream)
                  : launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false,
                                       d_ctl, d_ctl + 2, kBarrierLimitNs, stream);
         cudaError_t e2 = cudaStreamEndCapture(stream, &g);
@@ -307,6 +309,7 @@ struct qs_state {
     if (use_jit) {
       c.r = jit_lr;
       c.m = std::max(c.r, std::min(cfg.m, n));
+      c.pair_bit = jit_packed != 0;  // packed kernels: local bit 0 in every phase's registers
     }
     // The plan depends on the gate classes and bits only, not on the matrix values:
     // repeated circuits (parameter sweeps, benchmark steps) reuse it.
@@ -314,6 +317,7 @@ struct qs_state {
     auto mix = [&key](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
     mix((uint64_t)n); mix((uint64_t)dtype); mix((uint64_t)c.m); mix((uint64_t)c.k); mix((uint64_t)c.hill_iters);
     mix((uint64_t)c.r);
+    mix((uint64_t)c.pair_bit);
     for (const COp& o : cops) mix(((uint64_t)o.kind << 16) | ((uint64_t)(o.a & 0xff) << 8) | (uint64_t)(o.b & 0xff));
     const std::vector<PlannedPass>* passes = nullptr;
     for (auto& e : plan_cache)
@@ -359,7 +363,7 @@ struct qs_state {
     CK(cudaStreamSynchronize(stream));
     if (w[2] != 0) {
       CK(cudaMemsetAsync(d_ctl, 0, 3 * sizeof(unsigned), stream));
-      throw InvalidArg{"device error: a grid barrier wait expired (error word " + std::to_string(w[2]) + ")"};
+      throw InvalidArg{"device error: a bounded device wait expired (error word " + std::to_string(w[2]) + ")"};
     }
   }
 
@@ -715,7 +719,8 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     if (c->k < 1 || c->k > c->m) throw InvalidArg{"config: k out of range"};
     if (c->hill_iters < 0) throw InvalidArg{"config: hill_iters must be >= 0"};
     if (c->jit_lr < 3 || c->jit_lr > 5 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
-    if (c->jit_blocks < 1 || c->jit_blocks > 2) throw InvalidArg{"config: jit_blocks must be 1 or 2"};
+    if (c->jit_blocks < 1 || c->jit_blocks > 3) throw InvalidArg{"config: jit_blocks must be 1, 2 or 3"};
+    if (c->jit_packed < 0 || c->jit_packed > 1) throw InvalidArg{"config: jit_packed must be 0 or 1"};
     s->flush();
     s->cfg.m = c->m;
     s->cfg.k = c->k;
@@ -724,6 +729,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     s->jit_mode = c->jit;
     s->jit_lr = c->jit_lr;
     s->jit_blocks = c->jit_blocks;
+    s->jit_packed = c->jit_packed;
   });
 }
 
@@ -734,6 +740,7 @@ int qs_get_config(qs_state* s, qs_config* c) {
     c->jit = s->jit_mode;
     c->jit_lr = s->jit_lr;
     c->jit_blocks = s->jit_blocks;
+    c->jit_packed = s->jit_packed;
   });
 }
 
@@ -936,11 +943,13 @@ int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cf
     for (auto& o : q) c.push_back(classify(o));
     PlanConfig pc = cfg_from(0, num_qubits, cfg);
     pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) ? cfg->jit_lr : 5;
+    pc.pair_bit = cfg && cfg->jit_packed == 1;
     auto passes = plan_passes(c, num_qubits, pc);
     Program prog = build_program(q, passes, num_qubits, 0, pc.r);
     std::string log;
     JitConfig jc;
-    if (cfg && (cfg->jit_blocks == 1 || cfg->jit_blocks == 2)) jc.blocks = cfg->jit_blocks;
+    if (cfg && cfg->jit_blocks >= 1 && cfg->jit_blocks <= 3) jc.blocks = cfg->jit_blocks;
+    jc.packed = cfg && cfg->jit_packed == 1;
     const bool ok = jit_compile_check(prog, &log, jc);
     if (logbuf && logcap > 0) {
       const size_t k = std::min<size_t>(log.size(), (size_t)logcap - 1);

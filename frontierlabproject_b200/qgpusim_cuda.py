@@ -287,11 +287,12 @@ class _StatevectorBase:
         N.call("qs_reset_stats", self._h)
 
     def set_config(self, m: int = None, k: int = None, hill_iters: int = None, grid_mult: int = None,
-                   jit: int = None, jit_lr: int = None, jit_blocks: int = None) -> None:
+                   jit: int = None, jit_lr: int = None, jit_blocks: int = None, jit_packed: int = None) -> None:
         """Executor knobs: staged bits per sweep ``m``, always-staged low bits ``k``, planner
         effort ``hill_iters``, blocks per SM ``grid_mult``, specialised kernels ``jit``
-        (0 auto, 1 always, -1 never) with ``jit_lr`` register bits per thread and
-        ``jit_blocks`` resident blocks per SM."""
+        (0 auto, 1 always, -1 never) with ``jit_lr`` register bits per thread,
+        ``jit_blocks`` geometry (1 double-buffered block per SM, 2 single-buffered blocks per
+        SM, 3 one block of two teams over three buffers) and ``jit_packed`` FP32x2 arithmetic."""
         c = N.QsConfig()
         N.call("qs_get_config", self._h, byref(c))
         if jit is not None:
@@ -300,6 +301,8 @@ class _StatevectorBase:
             c.jit_lr = jit_lr
         if jit_blocks is not None:
             c.jit_blocks = jit_blocks
+        if jit_packed is not None:
+            c.jit_packed = jit_packed
         if m is not None:
             c.m = m
         if k is not None:
@@ -314,7 +317,7 @@ class _StatevectorBase:
         c = N.QsConfig()
         N.call("qs_get_config", self._h, byref(c))
         return {"m": c.m, "k": c.k, "hill_iters": c.hill_iters, "grid_mult": c.grid_mult, "jit": c.jit,
-                "jit_lr": c.jit_lr, "jit_blocks": c.jit_blocks}
+                "jit_lr": c.jit_lr, "jit_blocks": c.jit_blocks, "jit_packed": c.jit_packed}
 
     def device_ptr(self) -> int:
         p = c_void_p()

@@ -63,7 +63,9 @@ typedef struct {
   int jit;        /* plan-time specialised kernels in graphed mode: 0 auto (complex64,
                      >= 20 qubits), 1 always (complex64), -1 never */
   int jit_lr;     /* register bits per thread of the specialised kernels (3..5) */
-  int jit_blocks; /* resident blocks per SM of the specialised kernels (1 or 2) */
+  int jit_blocks; /* specialised kernels: 1 double-buffered block per SM, 2 single-buffered
+                     blocks per SM, 3 one block of two teams over three buffers */
+  int jit_packed; /* specialised kernels: FP32x2 arithmetic on two amplitudes (1) or scalar (0) */
 } qs_config;
 
 typedef struct {

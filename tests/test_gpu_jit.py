@@ -33,19 +33,20 @@ def test_jit_source_compiles_for_sm100a(native_lib):
             assert line.strip().startswith("0 bytes stack frame") or " 0 bytes spill stores" in line, line
 
 
-def _run_jit(qc, nl, **kw):
+def _run_jit(qc, nl, blocks=2, packed=0, **kw):
     _, plan = tile_circuit(qc, nl)
     sv = StatevectorF32(qc.num_qubits)
-    sv.set_config(jit=1)
+    sv.set_config(jit=1, jit_blocks=blocks, jit_packed=packed)
     psi, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv, **kw)
     return psi, met, plan, sv
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("blocks,packed", [(1, 0), (2, 0), (3, 0), (2, 1), (3, 1)])
 @pytest.mark.parametrize("n", [9, 13, 16])
-def test_jit_mixed_gates(n):
+def test_jit_mixed_gates(n, blocks, packed):
     qc = _mixed(n, n + 1)
-    psi, met, plan, sv = _run_jit(qc, max(4, n - 3), logical_order=True)
+    psi, met, plan, sv = _run_jit(qc, max(4, n - 3), blocks, packed, logical_order=True)
     assert O.infidelity(O.simulate(qc), psi) <= 1e-5
     assert np.max(np.abs(psi - O.simulate(qc))) <= 1e-5
     assert sv.stats()["graph_builds"] >= 1
@@ -124,10 +125,24 @@ def _flip_frame_circuit(n, seed):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("blocks,packed", [(2, 0), (3, 0), (2, 1)])
 @pytest.mark.parametrize("n,seed", [(16, 1), (20, 2)])
-def test_jit_flip_frame(n, seed):
+def test_jit_flip_frame(n, seed, blocks, packed):
     qc = _flip_frame_circuit(n, seed)
-    psi, _, _, _ = _run_jit(qc, n - 2, logical_order=True)
+    psi, _, _, _ = _run_jit(qc, n - 2, blocks, packed, logical_order=True)
     ref = O.simulate(qc)
     assert O.infidelity(ref, psi) <= 1e-5
     assert np.max(np.abs(psi - ref)) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [21, 24])
+def test_jit_teams_equal_single_team_bitwise(n):
+    # the two-team schedule (three rotating buffers, many groups per block at n=24) runs the
+    # same per-amplitude arithmetic as one team per block: identical bits
+    qc = C.random_layered(n, 12, 5)
+    psi2, _, _, _ = _run_jit(qc, n - 6, 2)
+    psi3, _, _, sv = _run_jit(qc, n - 6, 3)
+    assert sv.get_config()["jit_blocks"] == 3
+    np.testing.assert_array_equal(psi3.view(np.uint32), psi2.view(np.uint32))
+    assert abs(np.vdot(psi3.astype(np.complex128), psi3).real - 1.0) <= 1e-4
