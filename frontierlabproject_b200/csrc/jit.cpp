@@ -828,11 +828,11 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
         << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};";
     if (teams)
-      G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << ">(ex,prog,psi," << p << ",err,"
+      G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p << ",err,"
           << kDeviceWaitLimitNs << "ull);}\n";
     else
-      G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false")
-          << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,err,0ull);}\n";
+      G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false") << ","
+          << pd.nphase << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,err,0ull);}\n";
   }
   return G.o.str();
 }

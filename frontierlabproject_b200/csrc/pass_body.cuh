@@ -349,13 +349,13 @@ __device__ __forceinline__ void pass_setup(PassShared& sh, const uint8_t* __rest
 // flipped addresses); ex.reg_offsets(ph, h, B8) gives the swizzled byte offset of each
 // register bit of phase h.
 //
-// The phases of one group in the buffer at byte `bsel` (buffers start one bit above every
+// Phase h of one group in the buffer at byte `bsel` (buffers start one bit above every
 // swizzled byte offset of a group, so addresses are XOR combinations indexing smem_raw
-// directly).  t: thread index within the team; *gbp: physical base of the group (shared);
-// bar(): the team's barrier, after every phase.
-template <typename Real, int LR, typename Exec, typename Bar>
-__device__ __forceinline__ void group_phases(const Exec& ex, const uint8_t* __restrict__ prog, const PassShared& sh,
-                                             int p, uint32_t bsel, const uint64_t* gbp, unsigned t, const Bar& bar) {
+// directly).  t: thread index within the team (an active thread of the pass); *gbp: physical
+// base of the group (shared).
+template <typename Real, int LR, typename Exec>
+__device__ __forceinline__ void group_phase(const Exec& ex, const uint8_t* __restrict__ prog, const PassShared& sh,
+                                            int p, int h, uint32_t bsel, const uint64_t* gbp, unsigned t) {
   using C = typename V2<Real>::T;
   constexpr int NR = 1 << LR;
   constexpr bool kC64 = sizeof(Real) == 4;
@@ -364,54 +364,69 @@ __device__ __forceinline__ void group_phases(const Exec& ex, const uint8_t* __re
   const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
   const PassDesc& pd = sh.pd;
   const int nt = pd.m - pd.r;
-  const bool active = (int)t < (1 << nt);
-  for (int h = 0; h < pd.nphase; ++h) {
-    if (active) {
-      const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
-      uint32_t sb;
-      uint64_t pb = *gbp;
-      if (h < kPhaseTab) {
-        const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
-        sb = swz<Real>(sh.lt[e0] | sh.lt[e1]);
-        pb |= sh.pt[e0] | sh.pt[e1];
-      } else {
-        uint32_t lb = 0;
-        for (int j = 0; j < nt; ++j)
-          if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
-        sb = swz<Real>(lb);
-      }
-      uint32_t sb8 = bsel ^ (sb * kEsz);
-      uint32_t B8[LR];  // byte offset of register bit j (swizzled)
-      ex.template reg_offsets<Real, LR>(ph, h, B8);
-      if constexpr (Exec::kPacked) {
-        float2 R[NR / 2], I[NR / 2];
-        if (h == 0) packed_load<LR>(R, I, smem_raw, sb8, B8, true);
-        else packed_load<LR>(R, I, smem_raw, sb8, B8, false);
-        const uint32_t fl = ex.template run_packed<LR>(prog, h, R, I, pb);
-        sb8 ^= swz<Real>(fl & ~1u) * kEsz;
-        opaque(sb8);
+  const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+  uint32_t sb;
+  uint64_t pb = *gbp;
+  if (h < kPhaseTab) {
+    const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
+    sb = swz<Real>(sh.lt[e0] | sh.lt[e1]);
+    pb |= sh.pt[e0] | sh.pt[e1];
+  } else {
+    uint32_t lb = 0;
+    for (int j = 0; j < nt; ++j)
+      if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
+    sb = swz<Real>(lb);
+  }
+  uint32_t sb8 = bsel ^ (sb * kEsz);
+  uint32_t B8[LR];  // byte offset of register bit j (swizzled)
+  ex.template reg_offsets<Real, LR>(ph, h, B8);
+  if constexpr (Exec::kPacked) {
+    float2 R[NR / 2], I[NR / 2];
+    if (h == 0) packed_load<LR>(R, I, smem_raw, sb8, B8, true);
+    else packed_load<LR>(R, I, smem_raw, sb8, B8, false);
+    const uint32_t fl = ex.template run_packed<LR>(prog, h, R, I, pb);
+    sb8 ^= swz<Real>(fl & ~1u) * kEsz;
+    opaque(sb8);
 #pragma unroll
-        for (int j = 0; j < LR; ++j) opaque(B8[j]);
-        if (fl & 1u) packed_store<LR>(R, I, smem_raw, sb8, B8, true);  // warp-uniform
-        else packed_store<LR>(R, I, smem_raw, sb8, B8, false);
-      } else {
-        // register bit holding local bit 0 (complex64): its pairs are 16-byte accesses
-        const int jr = kC64 ? ex.template pair_reg<LR>(ph, h) : -1;
-        C a[NR];
-        regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, false, false);
-        // fl: local bits whose values the phase left flipped in the registers
-        const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
-        // a flipped local bit 0 swaps the halves of each 16-byte pair instead
-        const bool swap_pairs = jr >= 0 && (fl & 1u);
-        sb8 ^= swz<Real>(jr >= 0 ? (fl & ~1u) : fl) * kEsz;
-        opaque(sb8);
+    for (int j = 0; j < LR; ++j) opaque(B8[j]);
+    if (fl & 1u) packed_store<LR>(R, I, smem_raw, sb8, B8, true);  // warp-uniform
+    else packed_store<LR>(R, I, smem_raw, sb8, B8, false);
+  } else {
+    // register bit holding local bit 0 (complex64): its pairs are 16-byte accesses
+    const int jr = kC64 ? ex.template pair_reg<LR>(ph, h) : -1;
+    C a[NR];
+    regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, false, false);
+    // fl: local bits whose values the phase left flipped in the registers
+    const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
+    // a flipped local bit 0 swaps the halves of each 16-byte pair instead
+    const bool swap_pairs = jr >= 0 && (fl & 1u);
+    sb8 ^= swz<Real>(jr >= 0 ? (fl & ~1u) : fl) * kEsz;
+    opaque(sb8);
 #pragma unroll
-        for (int j = 0; j < LR; ++j) opaque(B8[j]);
-        if (swap_pairs) regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, true);  // warp-uniform
-        else regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, false);
-      }
+    for (int j = 0; j < LR; ++j) opaque(B8[j]);
+    if (swap_pairs) regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, true);  // warp-uniform
+    else regs_io<C, LR, 0>(jr, a, smem_raw, sb8, B8, true, false);
+  }
+}
+
+// All phases of one group; bar(): the team's barrier, after every phase.  NPH > 0: the pass's
+// phase count, known when the kernel is compiled (the loop unrolls, and the phase index, its
+// register offsets and its gate code become constants).
+template <typename Real, int LR, typename Exec, int NPH, typename Bar>
+__device__ __forceinline__ void group_phases(const Exec& ex, const uint8_t* __restrict__ prog, const PassShared& sh,
+                                             int p, uint32_t bsel, const uint64_t* gbp, unsigned t, const Bar& bar) {
+  const bool active = (int)t < (1 << (sh.pd.m - sh.pd.r));
+  if constexpr (NPH > 0) {
+#pragma unroll
+    for (int h = 0; h < NPH; ++h) {
+      if (active) group_phase<Real, LR>(ex, prog, sh, p, h, bsel, gbp, t);
+      bar();
     }
-    bar();
+  } else {
+    for (int h = 0; h < sh.pd.nphase; ++h) {
+      if (active) group_phase<Real, LR>(ex, prog, sh, p, h, bsel, gbp, t);
+      bar();
+    }
   }
 }
 
@@ -465,7 +480,7 @@ __device__ __forceinline__ void group_store(const PassShared& sh, typename V2<Re
 // One team per block.  kDouble: two group buffers per block (the next group's copies overlap
 // this group's phases); otherwise one buffer and two resident blocks per SM overlap each
 // other.
-template <typename Real, int LR, typename Exec, bool kDouble = true>
+template <typename Real, int LR, typename Exec, bool kDouble = true, int NPH = 0>
 __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restrict__ prog,
                                           typename V2<Real>::T* __restrict__ psi,
                                           int pass_begin, int pass_end, unsigned* bar, unsigned* err,
@@ -513,7 +528,7 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
         cp_async_wait<0>();
       }
       __syncthreads();
-      group_phases<Real, LR>(ex, prog, sh, p, bsel, &s_gb[it & 1], t, block_bar);
+      group_phases<Real, LR, Exec, NPH>(ex, prog, sh, p, bsel, &s_gb[it & 1], t, block_bar);
       group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[it & 1], t);
       __syncthreads();
     }
@@ -528,7 +543,7 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
 // s % 3; after finishing slot s a team copies slot s + 3 into buffer s % 3 for the other team.
 // Team 0 then waits at slot 2k for team 1's slot 2k - 3, team 1 at slot 2k + 1 for team 0's
 // slot 2k - 2: the teams alternate, and each group's copies run while both teams compute.
-template <typename Real, int LR, typename Exec>
+template <typename Real, int LR, typename Exec, int NPH = 0>
 __device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* __restrict__ prog,
                                                 typename V2<Real>::T* __restrict__ psi, int p, unsigned* err,
                                                 uint64_t limit_ns) {
@@ -580,7 +595,7 @@ __device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* _
     }
     (void)mbar_test(&s_mbar[b], parity);  // completed: acquires the copies for this thread
     const uint32_t bsel = b * bufb;
-    group_phases<Real, LR>(ex, prog, sh, p, bsel, &s_gb[team], t, team_bar);
+    group_phases<Real, LR, Exec, NPH>(ex, prog, sh, p, bsel, &s_gb[team], t, team_bar);
     group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[team], t);
     team_bar();  // buffer b is free
     if (group_of(s + 3) < ngroups) load_slot(s + 3);
