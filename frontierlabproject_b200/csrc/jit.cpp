@@ -766,6 +766,19 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         if (jr >= 0) G.o << "case " << h << ":return " << jr << ";";
       }
       G.o << "default:return -1;}}\n";
+      // physical offset (amplitudes) and local bit of each register bit per phase (the last
+      // phase stores straight to global memory)
+      G.o << "template<int LR>__device__ __forceinline__ void phys_offsets(int h,uint64_t (&P)[LR],uint32_t (&L)[LR])"
+          << "const{switch(h){";
+      for (int h = 0; h < pd.nphase; ++h) {
+        const PhaseDesc& ph = phs[pd.phase0 + h];
+        G.o << "case " << h << ":";
+        for (int j = 0; j < pd.r; ++j)
+          G.o << "P[" << j << "]=" << (1ull << pd.sbit[ph.rbit[j]]) << "ull;L[" << j << "]=" << (1u << ph.rbit[j])
+              << "u;";
+        G.o << "break;";
+      }
+      G.o << "default:break;}}\n";
       G.o << "template<typename C,int LR>__device__ __forceinline__ uint32_t run("
           << "const uint8_t* prog,const qsb::PhaseDesc*,int,int h,C (&a)[1<<LR],uint64_t pb)const{constexpr int NR=1<<LR;"
           << "const float2* K=(const float2*)(prog+((const qsb::ProgramHeader*)prog)->off_coef);switch(h){\n";
@@ -830,6 +843,9 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     if (teams)
       G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p << ",err,"
           << kDeviceWaitLimitNs << "ull);}\n";
+    else if (cfg.blocks == 2 && !packed && (1 << (pd.m - pd.r)) == hdr->max_threads)
+      G.o << "qsb::pass_body_direct<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p
+          << ");}\n";
     else
       G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false") << ","
           << pd.nphase << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,err,0ull);}\n";

@@ -156,8 +156,9 @@ constexpr int kPassThreads = 256;
 // Issue the asynchronous load of the group with physical base `gbase` into the shared buffer
 // `buf` (16-byte copies, swizzled destinations).  Items: c64 -> two amplitudes (local bit 0
 // inside the vector), c128 -> one amplitude.  `tbase` = physical offset of thread t's first
-// item.
-template <typename Real>
+// item.  kUnroll = false: one copy's address at a time (few registers, for copies issued while
+// a phase holds its amplitudes).
+template <typename Real, bool kUnroll = true>
 __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const typename V2<Real>::T* psi,
                                                uint64_t gbase, uint64_t tbase, const uint64_t* pv, int T, int V,
                                                unsigned t) {
@@ -165,7 +166,7 @@ __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const 
   if ((int)t >= T) return;
   const uint32_t lt = (uint32_t)t << kItemBits;
   const uint64_t base = gbase | tbase;
-#pragma unroll
+#pragma unroll(kUnroll ? 16 : 1)
   for (int v = 0; v < 16; ++v) {
     if (v >= V) break;
     const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << kItemBits);
@@ -535,6 +536,121 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
     cp_async_wait<0>();
     __syncthreads();
   }
+}
+
+// Last phase of a group (complex64, interleaved registers), stored from registers straight to
+// global memory: once the phase's loads are done every thread of the block has read the
+// buffer, so next() (the copies of the block's next group) is issued before the gates run, and
+// the copies overlap the gate arithmetic and the stores.  Every thread of the block is an
+// active thread of the pass (one block barrier inside).  ex.phys_offsets(h, P, L): physical
+// offset (in amplitudes) of register bit j and the local bit it holds.  Register i, left
+// holding the amplitude of register index i ^ (flipped bits), is written there.
+template <typename Real, int LR, typename Exec, typename Next>
+__device__ __forceinline__ void group_phase_direct(const Exec& ex, const uint8_t* __restrict__ prog,
+                                                   const PassShared& sh, int p, int h, const uint64_t* gbp,
+                                                   unsigned t, typename V2<Real>::T* __restrict__ psi,
+                                                   const Next& next) {
+  static_assert(sizeof(Real) == 4, "complex64 only");
+  using C = float2;
+  constexpr int NR = 1 << LR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const ProgramHeader* hdr = reinterpret_cast<const ProgramHeader*>(prog);
+  const PassDesc& pd = sh.pd;
+  const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(prog + hdr->off_phase) + pd.phase0 + h;
+  uint32_t sb;
+  uint64_t pb = *gbp;
+  if (h < kPhaseTab) {
+    const int e0 = h * 48 + (int)(t & 15u), e1 = h * 48 + 16 + (int)((t >> 4) & 31u);
+    sb = swz64(sh.lt[e0] | sh.lt[e1]);
+    pb |= sh.pt[e0] | sh.pt[e1];
+  } else {
+    uint32_t lb = 0;
+    for (int j = 0; j < pd.m - pd.r; ++j)
+      if ((t >> j) & 1u) { lb |= 1u << ph->tbit[j]; pb |= 1ull << pd.sbit[ph->tbit[j]]; }
+    sb = swz64(lb);
+  }
+  uint32_t B8[LR];
+  ex.template reg_offsets<Real, LR>(ph, h, B8);
+  const int jr = ex.template pair_reg<LR>(ph, h);
+  C a[NR];
+  regs_io<C, LR, 0>(jr, a, smem_raw, sb * 8u, B8, false, false);
+  __syncthreads();  // the buffer is free
+  next();
+  const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
+  uint64_t P[LR];
+  uint32_t L[LR];
+  ex.template phys_offsets<LR>(h, P, L);
+  uint64_t base = pb;
+#pragma unroll
+  for (int j = 0; j < LR; ++j)
+    if (j != jr && (fl & L[j])) base |= P[j];
+  opaque(base);
+  const bool swap = jr >= 0 && (fl & 1u);  // local bit 0 flipped: the halves of each pair swap
+  if (jr >= 0) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+      if ((i >> jr) & 1) continue;
+      uint64_t off = 0;
+#pragma unroll
+      for (int j = 0; j < LR; ++j)
+        if (j != jr && ((i >> j) & 1)) off |= P[j];
+      const int i1 = i | (1 << jr);
+      const C lo = swap ? a[i1] : a[i], hi = swap ? a[i] : a[i1];
+      __stcg(reinterpret_cast<float4*>(psi + (base ^ off)), make_float4(lo.x, lo.y, hi.x, hi.y));
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+      uint64_t off = 0;
+#pragma unroll
+      for (int j = 0; j < LR; ++j)
+        if ((i >> j) & 1) off |= P[j];
+      __stcg(psi + (base ^ off), a[i]);
+    }
+  }
+}
+
+// One pass per launch, one group buffer per block (two resident blocks per SM), complex64 with
+// interleaved registers, NPH phases known at compile time and every thread of the block active
+// in the pass: the last phase stores to global memory itself (group_phase_direct), so each
+// group's copies are issued during the previous group's last phase.
+template <typename Real, int LR, typename Exec, int NPH>
+__device__ __forceinline__ void pass_body_direct(const Exec& ex, const uint8_t* __restrict__ prog,
+                                                 typename V2<Real>::T* __restrict__ psi, int p) {
+  static_assert(NPH > 0, "phase count known at compile time");
+  using C = typename V2<Real>::T;
+  constexpr int kItemBits = sizeof(Real) == 4 ? 1 : 0;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ PassShared sh;
+  __shared__ uint64_t s_gb;  // physical base of the current group
+  const unsigned t = threadIdx.x;
+  pass_setup<Real>(sh, prog, p);
+  // copies of group gg (sizes and the thread's base re-read from shared memory: nothing of
+  // the copies stays live in registers across the last phase)
+  auto copy_group = [&](uint64_t gg) {
+    const int m = sh.pd.m, r = sh.pd.r;
+    const int T = 1 << (m - r);
+    if (gg < (1ull << sh.pd.ngbits) && (int)t < T)
+      prefetch_group<Real, false>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(gg, sh.gtab), sh.base[t], sh.pv,
+                                  T, 1 << (m - kItemBits) >> (m - r), t);
+    cp_async_commit();
+  };
+  const uint64_t ngroups = 1ull << sh.pd.ngbits;
+  uint64_t g = blockIdx.x;
+  copy_group(g);
+  for (; g < ngroups; g += gridDim.x) {
+    if (t == 0) s_gb = gbase_of(g, sh.gtab);  // the previous group's reads of s_gb are done
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < NPH - 1; ++h) {
+      group_phase<Real, LR>(ex, prog, sh, p, h, 0u, &s_gb, t);
+      __syncthreads();
+    }
+    group_phase_direct<Real, LR>(ex, prog, sh, p, NPH - 1, &s_gb, t, psi,
+                                 [&] { copy_group(g + gridDim.x); });
+  }
+  cp_async_wait<0>();
 }
 
 // Two teams of blockDim.x / 2 threads per block, three group buffers of 2^m amplitudes

@@ -447,16 +447,18 @@ static uint64_t fnv(uint64_t h, const void* p, size_t n) {
 
 // Thread-bit order: the first five (the lane bits) cover as many shared-memory bank
 // classes as possible, given the swizzle of the dtype.
-std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid) {
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid, uint64_t prefer) {
   auto cls = [&](int j) {
     if (dtype == 0) return j == 0 ? 0 : 1 + (j - 1) % 3;
     return j % 3;
   };
-  // candidates in preference order: bits outside `avoid` first
+  // candidates in preference order: `prefer`, then bits outside `avoid`, then the rest
   std::vector<int> rest;
+  for (int j : tb)
+    if ((prefer >> j) & 1ull) rest.push_back(j);
   for (int pass = 0; pass < 2; ++pass)
     for (int j : tb)
-      if (((avoid >> j) & 1ull) == (uint64_t)pass) rest.push_back(j);
+      if (!((prefer >> j) & 1ull) && ((avoid >> j) & 1ull) == (uint64_t)pass) rest.push_back(j);
   std::vector<int> out;
   std::vector<bool> covered(4, false);
   for (int c = 0; c < 4 && out.size() < 5; ++c) {
@@ -523,7 +525,10 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
         for (int j = 0; j < d.m; ++j)
           if (ps.sbits[j] == o.a && !(Rl & bit(j))) avoid |= bit(j);
       }
-      tb = order_thread_bits(tb, dtype, avoid);
+      // the pass's last phase: lanes over local bits 0-2 (the lowest physical bits), so its
+      // registers can be stored to global memory in contiguous 64-byte runs
+      const bool last = &ph == &ps.phases.back();
+      tb = order_thread_bits(tb, dtype, avoid, last ? 7ull : 0ull);
       for (size_t j = 0; j < tb.size(); ++j) h.tbit[j] = (int8_t)tb[j];
       h.gate0 = (int)gi.size();
       h.ngate = (int)ph.ops.size();

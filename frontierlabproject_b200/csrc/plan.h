@@ -62,8 +62,8 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
 
 // Order of a phase's thread bits (local bits not in registers): the lowest five (the lane
 // bits) cover as many shared-memory bank classes of the dtype's swizzle as possible, taking
-// bits outside `avoid` (a mask of local bits) first.
-std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid = 0);
+// bits of `prefer`, then bits outside `avoid` (masks of local bits) first.
+std::vector<int> order_thread_bits(const std::vector<int>& tb, int dtype, uint64_t avoid = 0, uint64_t prefer = 0);
 
 // In-place bit permutation as a sequence of gate-free passes.  perm[b] = destination
 // physical bit of the data now at physical bit b.
