@@ -836,8 +836,9 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     // are the by-value parameter kp (constant bank): the arithmetic reads them as operands,
     // with no load instruction and no register.
     const bool teams = cfg.blocks == 3;
+    const int per_sm = teams ? 1 : cfg.blocks == 4 ? 2 : cfg.blocks;  // resident blocks per SM
     G.o << "extern \"C\" __global__ void __launch_bounds__("
-        << (teams ? 2 : 1) * hdr->max_threads << "," << (teams ? 1 : cfg.blocks) << ") " << kname
+        << (teams ? 2 : 1) * hdr->max_threads << "," << per_sm << ") " << kname
         << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
         << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};";
     if (teams)
@@ -847,7 +848,7 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       G.o << "qsb::pass_body_direct<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p
           << ");}\n";
     else
-      G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks == 1 ? "true" : "false") << ","
+      G.o << "qsb::pass_body<float," << pd.r << ",X" << p << "," << (cfg.blocks != 2 ? "true" : "false") << ","
           << pd.nphase << ">(ex,prog,psi," << p << "," << p + 1 << ",nullptr,err,0ull);}\n";
   }
   return G.o.str();
@@ -1001,7 +1002,8 @@ cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const 
   void* args[] = {(void*)&d_prog, (void*)&psi, (void*)&err, const_cast<void*>(kp)};
   const unsigned smem = (unsigned)jit_smem_bytes(k.blocks, smem_double);
   const bool teams = k.blocks == 3;
-  CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)((teams ? 1 : k.blocks) * sms), 1, 1,
+  const int per_sm = teams ? 1 : k.blocks == 4 ? 2 : k.blocks;
+  CUresult r = driver().launch((CUfunction)k.functions[p], (unsigned)(per_sm * sms), 1, 1,
                                (unsigned)((teams ? 2 : 1) * threads), 1, 1, smem, (CUstream)stream, args, nullptr);
   if (r == CUDA_SUCCESS) return cudaSuccess;
   // launch-time rejections (configuration) are reported as such, not as a kernel failure

@@ -20,7 +20,8 @@ namespace qsb {
 // Geometry of the specialised kernels.  The register bits per thread (lr) are fixed when
 // the program is planned (2^(m - lr) threads per team); blocks = 1 double-buffers the
 // group loads inside a block, blocks = 2 gives each of two resident blocks one buffer,
-// blocks = 3 runs one block per SM of two teams over three buffers (pass_body_teams).
+// blocks = 3 runs one block per SM of two teams over three buffers (pass_body_teams), blocks = 4
+// two double-buffered blocks per SM.
 struct JitConfig {
   int blocks = 1;
   bool packed = true;   // FP32x2 registers for passes whose phases all hold local bit 0
@@ -62,7 +63,7 @@ cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const 
 
 // Dynamic shared memory of a specialised kernel: group buffers for the geometry.
 inline size_t jit_smem_bytes(int blocks, size_t smem_double) {
-  return blocks == 1 ? smem_double : blocks == 2 ? smem_double / 2 : smem_double / 2 * 3;
+  return blocks == 2 ? smem_double / 2 : blocks == 3 ? smem_double / 2 * 3 : smem_double;
 }
 
 // Compile a program's source on the host only (tests; returns the NVRTC log on failure).

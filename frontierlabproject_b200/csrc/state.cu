@@ -719,7 +719,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     if (c->k < 1 || c->k > c->m) throw InvalidArg{"config: k out of range"};
     if (c->hill_iters < 0) throw InvalidArg{"config: hill_iters must be >= 0"};
     if (c->jit_lr < 3 || c->jit_lr > 5 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
-    if (c->jit_blocks < 1 || c->jit_blocks > 3) throw InvalidArg{"config: jit_blocks must be 1, 2 or 3"};
+    if (c->jit_blocks < 1 || c->jit_blocks > 4) throw InvalidArg{"config: jit_blocks must be 1, 2, 3 or 4"};
     if (c->jit_packed < 0 || c->jit_packed > 1) throw InvalidArg{"config: jit_packed must be 0 or 1"};
     s->flush();
     s->cfg.m = c->m;
@@ -948,7 +948,7 @@ int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cf
     Program prog = build_program(q, passes, num_qubits, 0, pc.r);
     std::string log;
     JitConfig jc;
-    if (cfg && cfg->jit_blocks >= 1 && cfg->jit_blocks <= 3) jc.blocks = cfg->jit_blocks;
+    if (cfg && cfg->jit_blocks >= 1 && cfg->jit_blocks <= 4) jc.blocks = cfg->jit_blocks;
     jc.packed = cfg && cfg->jit_packed == 1;
     const bool ok = jit_compile_check(prog, &log, jc);
     if (logbuf && logcap > 0) {
