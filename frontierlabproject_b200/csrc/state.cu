@@ -899,7 +899,7 @@ static PlanConfig cfg_from(int dtype, int n, const qs_config* c) {
   p.r = reg_bits(dtype);
   p.m = c ? c->m : (dtype == 0 ? 13 : 12);
   p.k = c ? c->k : 3;
-  p.hill_iters = c ? c->hill_iters : 4;
+  p.hill_iters = c ? c->hill_iters : 16;
   p.m = std::max(p.r, std::min(p.m, n));
   return p;
 }
