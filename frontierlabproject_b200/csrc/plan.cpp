@@ -206,7 +206,8 @@ void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_op
 
 // ---------------------------------------------------------------------------------
 // Greedy + hill-climbing choice of a bit set of size `cap` (containing `forced`) that
-// executes the longest dependency-closed run of the remaining ops.
+// executes the longest dependency-closed run of the remaining ops; `restarts` perturbed
+// climbs from the best set found (iterated local search).
 // ---------------------------------------------------------------------------------
 namespace {
 
@@ -243,7 +244,7 @@ struct Scan {
 };
 
 uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candidates, uint64_t forced,
-                    int cap, int iters) {
+                    int cap, int iters, int restarts = 0) {
   uint64_t S = forced;
   // greedy seed in op order
   uint64_t blocked = 0;
@@ -263,19 +264,50 @@ uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candid
   }
   for (int p = 0; p < 64 && popc(S) < cap; ++p)
     if ((candidates & bit(p)) && !(S & bit(p))) S |= bit(p);
-  size_t best = sc.count(rem, S);
-  for (int it = 0; it < iters; ++it) {
-    bool improved = false;
-    for (int a = 0; a < 64 && !improved; ++a) {
-      if (!(S & bit(a)) || (forced & bit(a))) continue;
-      for (int b = 0; b < 64; ++b) {
-        if (!(candidates & bit(b)) || (S & bit(b))) continue;
-        uint64_t T = (S & ~bit(a)) | bit(b);
-        size_t c = sc.count(rem, T);
-        if (c > best) { best = c; S = T; improved = true; break; }
+  // first-improvement hill climbing over single-bit swaps (at most `iters` improvements)
+  auto climb = [&](uint64_t& X) {
+    size_t bx = sc.count(rem, X);
+    for (int it = 0; it < iters; ++it) {
+      bool improved = false;
+      for (int a = 0; a < 64 && !improved; ++a) {
+        if (!(X & bit(a)) || (forced & bit(a))) continue;
+        for (int b = 0; b < 64; ++b) {
+          if (!(candidates & bit(b)) || (X & bit(b))) continue;
+          uint64_t T = (X & ~bit(a)) | bit(b);
+          size_t c = sc.count(rem, T);
+          if (c > bx) { bx = c; X = T; improved = true; break; }
+        }
       }
+      if (!improved) break;
     }
-    if (!improved) break;
+    return bx;
+  };
+  size_t best = climb(S);
+  // iterated local search: restart the climb from the best set with three random bit swaps
+  // (a fixed xorshift sequence per call: plans are deterministic), keep strict improvements
+  uint64_t rng = 0x9E3779B97F4A7C15ull ^ ((uint64_t)rem.size() * 0xBF58476D1CE4E5B9ull);
+  auto next = [&rng]() {
+    rng ^= rng << 13;
+    rng ^= rng >> 7;
+    rng ^= rng << 17;
+    return rng;
+  };
+  std::vector<int> in, out;
+  for (int r = 0; r < restarts; ++r) {
+    uint64_t T = S;
+    for (int k = 0; k < 3; ++k) {
+      in.clear();
+      out.clear();
+      for (int p = 0; p < 64; ++p) {
+        if ((T & bit(p)) && !(forced & bit(p))) in.push_back(p);
+        else if ((candidates & bit(p)) && !(T & bit(p))) out.push_back(p);
+      }
+      if (in.empty() || out.empty()) break;
+      const int a = in[next() % in.size()], b = out[next() % out.size()];
+      T = (T & ~bit(a)) | bit(b);
+    }
+    const size_t c = climb(T);
+    if (c > best) { best = c; S = T; }
   }
   return S;
 }
@@ -332,7 +364,7 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
   std::vector<int> rem(ops.size()), taken, rest;
   for (size_t i = 0; i < ops.size(); ++i) rem[i] = (int)i;
   while (!rem.empty()) {
-    uint64_t S = (m == n) ? all : choose_set(sc, rem, all, forced, m, cfg.hill_iters);
+    uint64_t S = (m == n) ? all : choose_set(sc, rem, all, forced, m, cfg.hill_iters, cfg.hill_iters);
     sc.run(rem, S, taken);
     if (taken.empty()) throw std::runtime_error("planner: pass made no progress");
     PlannedPass ps;

@@ -41,7 +41,8 @@ struct PlanConfig {
   int m = 13;             // local bits per pass
   int r = 5;              // register bits per thread
   int k = 3;              // lowest physical bits always staged (contiguous runs of 2^k amplitudes)
-  int hill_iters = 16;    // hill-climbing rounds when choosing the staged / register sets
+  int hill_iters = 16;    // hill-climbing rounds when choosing the staged / register sets (and
+                          // restarts of the staged-set search)
   bool pair_bit = false;  // physical bit 0 is a register bit of every phase (packed kernels)
 };
 
