@@ -386,7 +386,8 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
 std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, const PlanConfig& cfg) {
   // perm[b] = destination bit of the data at bit b.  Cycles are packed into passes whose
   // staged set (always holding the k lowest bits) has at most m bits; a cycle longer than
-  // the free room is split: (c0 .. cL-1) = (c0 c_{j+1} .. c_{L-1}) after (c0 .. c_j).
+  // the free room is split: (c0 .. cL-1) = (c0 c_{j+1} .. c_{L-1}) after (c0 .. c_j), and
+  // the pieces are placed first-fit (each after its cycle's previous piece).
   std::vector<PlannedPass> out;
   const int m = std::min(cfg.m, n);
   const int k = std::min(cfg.k, m);
@@ -410,8 +411,9 @@ std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, c
   const int room = m - k;
   // split long cycles
   std::vector<std::vector<int>> fitted;
-  for (auto& c : pieces) {
-    std::vector<int> cyc = c;
+  std::vector<int> cyc_of;  // cycle index of each piece
+  for (size_t ci = 0; ci < pieces.size(); ++ci) {
+    std::vector<int> cyc = pieces[ci];
     while (extra(cyc) > room) {
       // take the longest prefix c0..cj with extra() <= room
       std::vector<int> head;
@@ -421,31 +423,31 @@ std::vector<PlannedPass> plan_permutation(const std::vector<int>& perm, int n, c
       }
       if (head.size() < 2) throw std::runtime_error("planner: cannot split permutation cycle");
       fitted.push_back(head);
+      cyc_of.push_back((int)ci);
       std::vector<int> tail;
       tail.push_back(cyc[0]);
       for (size_t i = head.size(); i < cyc.size(); ++i) tail.push_back(cyc[i]);
       cyc.swap(tail);
     }
-    if (cyc.size() >= 2) fitted.push_back(cyc);
+    if (cyc.size() >= 2) { fitted.push_back(cyc); cyc_of.push_back((int)ci); }
   }
-  // pack pieces in order into passes (pieces of one cycle stay in order; a piece that
-  // shares a position with the open pass starts a new pass)
+  // first fit: each piece joins the earliest pass after its cycle's previous piece whose
+  // positions it does not share and whose staged set keeps room
   std::vector<std::vector<std::vector<int>>> groups;
   std::vector<uint64_t> gmask;
-  for (auto& pc : fitted) {
+  std::vector<int> last_pass(pieces.size(), -1);
+  const uint64_t low = (k >= 64) ? ~0ull : (bit(k) - 1);
+  for (size_t pi = 0; pi < fitted.size(); ++pi) {
+    const auto& pc = fitted[pi];
     uint64_t pm = 0;
     for (int p : pc) pm |= bit(p);
-    bool placed = false;
-    if (!groups.empty()) {
-      uint64_t gm = gmask.back();
-      uint64_t hi = (gm | pm) & ~((k >= 64) ? ~0ull : (bit(k) - 1));
-      if (!(gm & pm) && popc(hi) <= room) {
-        groups.back().push_back(pc);
-        gmask.back() |= pm;
-        placed = true;
-      }
-    }
-    if (!placed) { groups.push_back({pc}); gmask.push_back(pm); }
+    int g = last_pass[cyc_of[pi]] + 1;
+    for (; g < (int)groups.size(); ++g)
+      if (!(gmask[g] & pm) && popc((gmask[g] | pm) & ~low) <= room) break;
+    if (g == (int)groups.size()) { groups.push_back({}); gmask.push_back(0); }
+    groups[g].push_back(pc);
+    gmask[g] |= pm;
+    last_pass[cyc_of[pi]] = g;
   }
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     uint64_t S = gmask[gi] | ((k >= 64) ? ~0ull : (bit(k) - 1));
