@@ -841,10 +841,12 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         << (teams ? 2 : 1) * hdr->max_threads << "," << per_sm << ") " << kname
         << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
         << "const __grid_constant__ KP" << p << " kp){const X" << p << " ex{&kp};";
+    const bool all_active = (1 << (pd.m - pd.r)) == hdr->max_threads;
     if (teams)
-      G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p << ",err,"
+      G.o << "qsb::pass_body_teams<float," << pd.r << ",X" << p << "," << pd.nphase << ","
+          << (!packed && all_active && pd.nphase > 0 ? "true" : "false") << ">(ex,prog,psi," << p << ",err,"
           << kDeviceWaitLimitNs << "ull);}\n";
-    else if (cfg.blocks == 2 && !packed && (1 << (pd.m - pd.r)) == hdr->max_threads)
+    else if (cfg.blocks == 2 && !packed && all_active && pd.nphase > 0)
       G.o << "qsb::pass_body_direct<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi," << p
           << ");}\n";
     else

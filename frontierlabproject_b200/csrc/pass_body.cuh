@@ -545,10 +545,11 @@ __device__ __forceinline__ void pass_body(const Exec& ex, const uint8_t* __restr
 // active thread of the pass (one block barrier inside).  ex.phys_offsets(h, P, L): physical
 // offset (in amplitudes) of register bit j and the local bit it holds.  Register i, left
 // holding the amplitude of register index i ^ (flipped bits), is written there.
-template <typename Real, int LR, typename Exec, typename Next>
+template <typename Real, int LR, typename Exec, typename Bar, typename Next>
 __device__ __forceinline__ void group_phase_direct(const Exec& ex, const uint8_t* __restrict__ prog,
-                                                   const PassShared& sh, int p, int h, const uint64_t* gbp,
-                                                   unsigned t, typename V2<Real>::T* __restrict__ psi,
+                                                   const PassShared& sh, int p, int h, uint32_t bsel,
+                                                   const uint64_t* gbp, unsigned t,
+                                                   typename V2<Real>::T* __restrict__ psi, const Bar& bar,
                                                    const Next& next) {
   static_assert(sizeof(Real) == 4, "complex64 only");
   using C = float2;
@@ -573,8 +574,8 @@ __device__ __forceinline__ void group_phase_direct(const Exec& ex, const uint8_t
   ex.template reg_offsets<Real, LR>(ph, h, B8);
   const int jr = ex.template pair_reg<LR>(ph, h);
   C a[NR];
-  regs_io<C, LR, 0>(jr, a, smem_raw, sb * 8u, B8, false, false);
-  __syncthreads();  // the buffer is free
+  regs_io<C, LR, 0>(jr, a, smem_raw, bsel ^ (sb * 8u), B8, false, false);
+  bar();  // the buffer is free
   next();
   const uint32_t fl = ex.template run<C, LR>(prog, ph, p, h, a, pb);
   uint64_t P[LR];
@@ -647,7 +648,7 @@ __device__ __forceinline__ void pass_body_direct(const Exec& ex, const uint8_t* 
       group_phase<Real, LR>(ex, prog, sh, p, h, 0u, &s_gb, t);
       __syncthreads();
     }
-    group_phase_direct<Real, LR>(ex, prog, sh, p, NPH - 1, &s_gb, t, psi,
+    group_phase_direct<Real, LR>(ex, prog, sh, p, NPH - 1, 0u, &s_gb, t, psi, [] { __syncthreads(); },
                                  [&] { copy_group(g + gridDim.x); });
   }
   cp_async_wait<0>();
@@ -659,7 +660,9 @@ __device__ __forceinline__ void pass_body_direct(const Exec& ex, const uint8_t* 
 // s % 3; after finishing slot s a team copies slot s + 3 into buffer s % 3 for the other team.
 // Team 0 then waits at slot 2k for team 1's slot 2k - 3, team 1 at slot 2k + 1 for team 0's
 // slot 2k - 2: the teams alternate, and each group's copies run while both teams compute.
-template <typename Real, int LR, typename Exec, int NPH = 0>
+// kDirect (complex64, NPH > 0, every thread of a team active): the last phase stores from
+// registers and issues the copies of slot s + 3 as soon as it has read buffer s % 3.
+template <typename Real, int LR, typename Exec, int NPH = 0, bool kDirect = false>
 __device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* __restrict__ prog,
                                                 typename V2<Real>::T* __restrict__ psi, int p, unsigned* err,
                                                 uint64_t limit_ns) {
@@ -690,6 +693,13 @@ __device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* _
                          sh.pv, T, V, t);
     cp_async_mbar_arrive(&s_mbar[b]);
   };
+  // the same, issued inside a last phase: one copy address at a time, the thread's base re-read
+  auto load_slot_rolled = [&](uint64_t s) {
+    const uint32_t b = (uint32_t)(s % 3u);
+    prefetch_group<Real, false>(reinterpret_cast<C*>(smem_raw + b * bufb), psi, gbase_of(group_of(s), sh.gtab),
+                                sh.base[t], sh.pv, T, V, t);
+    cp_async_mbar_arrive(&s_mbar[b]);
+  };
   auto team_bar = [team, TS] { named_barrier(1u + team, TS); };
   if (team == 0) {
     if (group_of(0) < ngroups) load_slot(0);
@@ -711,10 +721,22 @@ __device__ __forceinline__ void pass_body_teams(const Exec& ex, const uint8_t* _
     }
     (void)mbar_test(&s_mbar[b], parity);  // completed: acquires the copies for this thread
     const uint32_t bsel = b * bufb;
-    group_phases<Real, LR, Exec, NPH>(ex, prog, sh, p, bsel, &s_gb[team], t, team_bar);
-    group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[team], t);
-    team_bar();  // buffer b is free
-    if (group_of(s + 3) < ngroups) load_slot(s + 3);
+    if constexpr (kDirect) {
+      static_assert(NPH > 0, "phase count known at compile time");
+#pragma unroll
+      for (int h = 0; h < NPH - 1; ++h) {
+        group_phase<Real, LR>(ex, prog, sh, p, h, bsel, &s_gb[team], t);
+        team_bar();
+      }
+      group_phase_direct<Real, LR>(ex, prog, sh, p, NPH - 1, bsel, &s_gb[team], t, psi, team_bar, [&] {
+        if (group_of(s + 3) < ngroups) load_slot_rolled(s + 3);
+      });
+    } else {
+      group_phases<Real, LR, Exec, NPH>(ex, prog, sh, p, bsel, &s_gb[team], t, team_bar);
+      group_store<Real, Exec::kPacked>(sh, psi, bsel, s_gb[team], t);
+      team_bar();  // buffer b is free
+      if (group_of(s + 3) < ngroups) load_slot(s + 3);
+    }
   }
 }
 
