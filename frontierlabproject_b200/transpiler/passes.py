@@ -11,12 +11,16 @@ Restates the algorithms of qgpusim/transpiler/passes.py so that the schedule
 
 The gate list is handled as integer indices with a "removed" mask instead of the
 reference's per-gate list rebuild, so tiling a 4,500-gate circuit is linear per
-tile rather than quadratic.
+tile rather than quadratic.  ``run`` hands Alg. 1-3 and the tile extraction to the
+native library (``qs_lqr_flat_tiling``, the same algorithms on 64-bit qubit masks) when
+it loads and the circuit has at most 64 qubits; ``flat_tiling`` here is the Python
+statement of the same steps.
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
-from typing import Dict, List, Sequence, Set, Tuple
+from typing import Dict, List, Optional, Sequence, Set, Tuple
 
 from ..circuit import DAGCircuit, DAGOpNode
 
@@ -40,13 +44,30 @@ def _build_tile_layout(logical_qubits: Sequence[int], num_qubits: int) -> List[i
     return list(logical_qubits) + [q for q in range(num_qubits) if q not in local]
 
 
-class LazyQubitReordering:
-    """LQR pass.  ``run(dag)`` stores the tile plan in ``property_set["flat_tiling_plan"]``."""
+_NATIVE_OK: Optional[bool] = None
 
-    def __init__(self, nL: int):
+
+def _native_available() -> bool:
+    global _NATIVE_OK
+    if _NATIVE_OK is None:
+        try:
+            from .. import _native
+            _native.lib()
+            _NATIVE_OK = True
+        except Exception:  # library not built: the Python statement of the algorithms runs
+            _NATIVE_OK = False
+    return _NATIVE_OK
+
+
+class LazyQubitReordering:
+    """LQR pass.  ``run(dag)`` stores the tile plan in ``property_set["flat_tiling_plan"]``.
+    ``native``: None = the C++ tiler when the library loads, True / False = force it on / off."""
+
+    def __init__(self, nL: int, native: Optional[bool] = None):
         if nL < 1:
             raise ValueError("nL must be >= 1")
         self.nL = nL
+        self.native = native
         self.property_set: dict = {}
 
     # ---- Alg. 2 -------------------------------------------------------------------
@@ -135,6 +156,33 @@ class LazyQubitReordering:
                 QL = self._scan_mapping(set(Q), remaining, targets, nL)
         return schedule, M
 
+    @staticmethod
+    def flat_tiling_native(n: int, C: List, T_map: Dict, nL: int, tiles_out: Optional[list] = None
+                           ) -> Tuple[List, Dict]:
+        """``flat_tiling`` by the native library (qubit sets as 64-bit masks, n <= 64).  The
+        gates of one tile share one qubit set in M; tiles_out (optional) receives the
+        (qubit set, gates) pairs of ``extract_tiles``."""
+        import numpy as np
+        from .. import _native as N
+        nodes = list(C)
+        ng = len(nodes)
+        masks = np.fromiter((sum(1 << q for q in T_map[nd]) for nd in nodes), dtype=np.uint64, count=ng)
+        order = np.empty(max(ng, 1), np.int32)
+        tile_of = np.empty(max(ng, 1), np.int32)
+        tmasks = np.empty(max(ng, 1), np.uint64)
+        nt = ctypes.c_int()
+        N.call("qs_lqr_flat_tiling", n, nL, masks.ctypes.data, ng, order.ctypes.data, tile_of.ctypes.data,
+               tmasks.ctypes.data, ctypes.byref(nt))
+        sets = [{q for q in range(n) if (int(m) >> q) & 1} for m in tmasks[:nt.value]]
+        schedule = [nodes[i] for i in order[:ng].tolist()]
+        tl = tile_of[:ng].tolist()
+        M = {nd: sets[t] for nd, t in zip(schedule, tl)}
+        if tiles_out is not None:
+            tiles_out.extend((s, []) for s in sets)
+            for nd, t in zip(schedule, tl):
+                tiles_out[t][1].append(nd)
+        return schedule, M
+
     # ---- helpers ------------------------------------------------------------------
     @staticmethod
     def extract_tiles(g_schedule: List, M: Dict) -> List[Tuple[Set[int], List]]:
@@ -159,9 +207,11 @@ class LazyQubitReordering:
                 "max_Q_L_size": max(qls)}
 
     @staticmethod
-    def build_tiling_plan(g_schedule: List, M: Dict, num_qubits: int) -> List[Tile]:
+    def build_tiling_plan(g_schedule: List, M: Dict, num_qubits: int, tiles: Optional[list] = None) -> List[Tile]:
         plan: List[Tile] = []
-        for idx, (ql_set, gates) in enumerate(LazyQubitReordering.extract_tiles(g_schedule, M)):
+        if tiles is None:
+            tiles = LazyQubitReordering.extract_tiles(g_schedule, M)
+        for idx, (ql_set, gates) in enumerate(tiles):
             ql = sorted(ql_set)
             plan.append(Tile(tile_idx=idx, logical_qubits=ql,
                              global_to_local_map={gq: i for i, gq in enumerate(ql)},
@@ -183,10 +233,16 @@ class LazyQubitReordering:
                 last[i] = d
         nodes.sort(key=lambda nd: depth[nd])  # stable, as list.sort is
         T_map = {node: {qindex[q] for q in node.qargs} for node in nodes}
-        schedule, M = self.flat_tiling(set(range(n)), nodes, T_map, self.nL)
+        native = self.native if self.native is not None else _native_available()
+        tiles = None
+        if native and n <= 64:
+            tiles = []
+            schedule, M = self.flat_tiling_native(n, nodes, T_map, self.nL, tiles)
+        else:
+            schedule, M = self.flat_tiling(set(range(n)), nodes, T_map, self.nL)
         self.property_set["flat_tiling_schedule"] = schedule
         self.property_set["flat_tiling_mapping"] = M
-        self.property_set["flat_tiling_plan"] = self.build_tiling_plan(schedule, M, n)
+        self.property_set["flat_tiling_plan"] = self.build_tiling_plan(schedule, M, n, tiles)
         out = dag.copy_empty_like()
         for node in schedule:
             out.apply_operation_back(node.op, qargs=node.qargs, cargs=node.cargs)

@@ -1,7 +1,7 @@
 """Pass-manager factory, same signature as qgpusim/transpiler/pm.py:11-19."""
 from __future__ import annotations
 
-from typing import Tuple
+from typing import Optional, Tuple
 
 from ..circuit import QuantumCircuit, circuit_to_dag, dag_to_circuit
 from .passes import LazyQubitReordering
@@ -26,15 +26,16 @@ class PassManager:
         return dag_to_circuit(dag)
 
 
-def make_custom_pm(num_local_qubits: int) -> Tuple[PassManager, LazyQubitReordering]:
-    lqr_pass = LazyQubitReordering(num_local_qubits)
+def make_custom_pm(num_local_qubits: int, native: Optional[bool] = None) -> Tuple[PassManager, LazyQubitReordering]:
+    lqr_pass = LazyQubitReordering(num_local_qubits, native)
     pm = PassManager()
     pm.append(lqr_pass)
     return pm, lqr_pass
 
 
-def tile_circuit(qc: QuantumCircuit, num_local_qubits: int):
-    """Convenience: (tiled circuit, tile plan) for ``qc`` at ``nL = num_local_qubits``."""
-    pm, lqr = make_custom_pm(num_local_qubits)
+def tile_circuit(qc: QuantumCircuit, num_local_qubits: int, native: Optional[bool] = None):
+    """Convenience: (tiled circuit, tile plan) for ``qc`` at ``nL = num_local_qubits``
+    (``native``: the C++ tiler; None = when the library loads)."""
+    pm, lqr = make_custom_pm(num_local_qubits, native)
     tqc = pm.run(qc)
     return tqc, lqr.property_set["flat_tiling_plan"]

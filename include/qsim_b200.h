@@ -205,6 +205,15 @@ QS_API int qs_permute_scatter(const void* in, void* out, int dtype, int num_qubi
  * legacy default stream) has finished. */
 QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_op* ops, int nops, void* stream);
 
+/* LQR flat tiling of a depth-sorted gate list (host only; replaces the Python loops of
+ * LazyQubitReordering.flat_tiling / tile_construction / greedy_qubit_mapping and
+ * extract_tiles, qgpusim/transpiler/passes.py:89-272).  targets[i] = bit mask of gate i's
+ * qubits (num_qubits <= 64), in the order of passes.py:359-368's stable depth sort.  Out:
+ * order[k] = input index of the k-th scheduled gate, tile_of[k] = its tile, tile_masks[t] =
+ * the qubit set of tile t (room for ngates entries), *ntiles. */
+QS_API int qs_lqr_flat_tiling(int num_qubits, int nL, const unsigned long long* targets, int ngates, int* order,
+                              int* tile_of, unsigned long long* tile_masks, int* ntiles);
+
 /* Planner inspection (host only, no GPU needed): plan the ops of a tile list for an
  * n-qubit state and report sweeps / phases.  ops use physical bits. */
 QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg,

@@ -13,12 +13,45 @@ def _record(qc, plan):
              "gates": [pos[(id(g.op), tuple(g.qargs))] for g in t.gates]} for t in plan]
 
 
+@pytest.mark.parametrize("native", [False, True], ids=["python", "native"])
 @pytest.mark.parametrize("name", sorted(BUILDERS))
-def test_schedule_matches_reference(name, schedules):
+def test_schedule_matches_reference(name, native, schedules):
     qc = BUILDERS[name]()
     nL = nl_of(name)
-    _, plan = tile_circuit(qc, nL)
+    _, plan = tile_circuit(qc, nL, native=native)
     assert _record(qc, plan) == schedules[name]["tiles"]
+
+
+@pytest.mark.parametrize("n,depth,nL,seed", [(12, 10, 3, 1), (16, 20, 6, 2), (20, 30, 14, 3), (9, 15, 1, 4),
+                                             (24, 12, 24, 5), (30, 40, 20, 6)])
+def test_native_tiler_equals_python(n, depth, nL, seed):
+    # same tiles, same gates per tile, same mapping sets (forced tiles included at small nL)
+    from frontierlabproject_b200 import circuits as C
+    qc = C.random_layered(n, depth, seed)
+    qc.cx(0, n - 1)
+    qc.swap(1, n // 2)
+    out = {}
+    for native in (False, True):
+        pm, lqr = make_custom_pm(nL, native=native)
+        tqc = pm.run(qc)
+        plan = lqr.property_set["flat_tiling_plan"]
+        sched = lqr.property_set["flat_tiling_schedule"]
+        M = lqr.property_set["flat_tiling_mapping"]
+        out[native] = (_record(qc, plan), [(id(nd.op), tuple(nd.qargs)) for nd in sched],
+                       [sorted(M[nd]) for nd in sched], [ins.operation for ins in tqc.data])
+    assert out[True] == out[False]
+
+
+def test_native_tiler_rejects_bad_input(native_lib):
+    import ctypes
+    from frontierlabproject_b200 import _native as N
+    masks = (ctypes.c_ulonglong * 1)(1 << 5)
+    o, t, nt = (ctypes.c_int * 1)(), (ctypes.c_int * 1)(), ctypes.c_int()
+    tm = (ctypes.c_ulonglong * 1)()
+    with pytest.raises(RuntimeError, match="out of range"):
+        N.call("qs_lqr_flat_tiling", 4, 2, masks, 1, o, t, tm, ctypes.byref(nt))
+    with pytest.raises(RuntimeError, match="invalid argument"):
+        N.call("qs_lqr_flat_tiling", 4, 0, masks, 1, o, t, tm, ctypes.byref(nt))
 
 
 def test_published_tile_counts(schedules):
