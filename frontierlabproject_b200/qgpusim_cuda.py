@@ -54,8 +54,14 @@ class _OpBatch:
         n = len(ops)
         self.arr = np.zeros(n, dtype=N.OP_DTYPE)
         self._keep: List[np.ndarray] = []
+        kinds: List[int] = []
+        q0s: List[int] = []
+        q1s: List[int] = []
+        devs: List[int] = []
+        ptrs: List[int] = []
         host_mats = []
         host_idx = []
+        item = np.dtype(npdt).itemsize
         for i, op in enumerate(ops):
             t = tuple(op)
             if len(t) < 1:
@@ -64,16 +70,16 @@ class _OpBatch:
             if kind == "1q":
                 if len(t) != 3:
                     raise RuntimeError("apply_tile_dev: 1q expects ('1q', q0, U_dev)")
-                self.arr[i]["kind"] = N.QS_OP_1Q
-                self.arr[i]["q0"] = int(t[1])
-                self.arr[i]["q1"] = -1
+                kinds.append(N.QS_OP_1Q)
+                q0s.append(int(t[1]))
+                q1s.append(-1)
                 U, shape = t[2], (2, 2)
             elif kind == "2q":
                 if len(t) != 4:
                     raise RuntimeError("apply_tile_dev: 2q expects ('2q', q0, q1, U_dev)")
-                self.arr[i]["kind"] = N.QS_OP_2Q
-                self.arr[i]["q0"] = int(t[1])
-                self.arr[i]["q1"] = int(t[2])
+                kinds.append(N.QS_OP_2Q)
+                q0s.append(int(t[1]))
+                q1s.append(int(t[2]))
                 U, shape = t[3], (4, 4)
             else:
                 raise RuntimeError(f"apply_tile_dev: unknown op kind: {kind}")
@@ -82,24 +88,28 @@ class _OpBatch:
                 ptr, dshape, dts, strides = dev
                 if dts != typestr:
                     raise RuntimeError(f"apply_tile_dev: device matrix must have typestr {typestr}, got {dts}")
-                if dshape != shape or strides not in (None, (shape[1] * npdt().itemsize, npdt().itemsize)):
+                if dshape != shape or strides not in (None, (shape[1] * item, item)):
                     raise RuntimeError(f"U must be a contiguous {shape[0]}x{shape[1]} matrix")
-                self.arr[i]["dev"] = 1
-                self.arr[i]["U"] = ptr
+                devs.append(1)
+                ptrs.append(ptr)
                 self._keep.append(U)
             else:
-                host_mats.append(_host_matrix(U, npdt, shape, kind))
+                host_mats.append(_host_matrix(U, npdt, shape, kind).reshape(-1))
                 host_idx.append(i)
+                devs.append(0)
+                ptrs.append(0)
+        if n:
+            self.arr["kind"] = kinds
+            self.arr["q0"] = q0s
+            self.arr["q1"] = q1s
+            self.arr["dev"] = devs
+            self.arr["U"] = ptrs
         if host_mats:
-            sizes = [m.size for m in host_mats]
-            buf = np.empty(sum(sizes), dtype=npdt)
-            off = 0
-            base = buf.ctypes.data
-            item = buf.itemsize
-            for i, m, sz in zip(host_idx, host_mats, sizes):
-                buf[off:off + sz] = m.reshape(-1)
-                self.arr[i]["U"] = base + off * item
-                off += sz
+            # one buffer for all host matrices; each op points at its entries
+            buf = np.concatenate(host_mats)
+            sizes = np.fromiter((m.size for m in host_mats), dtype=np.uint64, count=len(host_mats))
+            offs = np.cumsum(sizes) - sizes  # entry offset of each matrix in buf
+            self.arr["U"][np.asarray(host_idx)] = np.uint64(buf.ctypes.data) + offs * np.uint64(item)
             self._keep.append(buf)
 
     @property
