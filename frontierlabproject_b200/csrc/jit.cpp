@@ -766,6 +766,19 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         if (jr >= 0) G.o << "case " << h << ":return " << jr << ";";
       }
       G.o << "default:return -1;}}\n";
+      // group copies: physical offset and swizzled byte offset of item row v of thread 0
+      {
+        const int T = 1 << (pd.m - pd.r), V = 1 << (pd.r - 1);
+        G.o << "template<int V>__device__ __forceinline__ void copy_offsets(uint64_t (&P)[V],uint32_t (&D)[V])const{";
+        for (int v = 0; v < V; ++v) {
+          const uint32_t lv = ((uint32_t)v * (uint32_t)T) << 1;
+          uint64_t q = 0;
+          for (int j = 0; j < pd.m; ++j)
+            if ((lv >> j) & 1u) q |= 1ull << pd.sbit[j];
+          G.o << "P[" << v << "]=" << q << "ull;D[" << v << "]=" << swz64(lv) * 8u << "u;";
+        }
+        G.o << "}\n";
+      }
       // physical offset (amplitudes) and local bit of each register bit per phase (the last
       // phase stores straight to global memory)
       G.o << "template<int LR>__device__ __forceinline__ void phys_offsets(int h,uint64_t (&P)[LR],uint32_t (&L)[LR])"

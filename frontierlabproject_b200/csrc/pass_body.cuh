@@ -626,14 +626,21 @@ __device__ __forceinline__ void pass_body_direct(const Exec& ex, const uint8_t* 
   __shared__ uint64_t s_gb;  // physical base of the current group
   const unsigned t = threadIdx.x;
   pass_setup<Real>(sh, prog, p);
-  // copies of group gg (sizes and the thread's base re-read from shared memory: nothing of
-  // the copies stays live in registers across the last phase)
+  // copies of group gg: row v of thread t is local index (t << 1) | lv_v, so (the deposit and
+  // the swizzle being linear) its source is (group base | thread base) | P[v] and its swizzled
+  // destination (swz(t << 1) * 8) ^ D[v], with P / D constants of the pass (ex.copy_offsets);
+  // the thread's base is re-read from shared memory, so nothing stays live across the last phase
+  constexpr int V = 1 << (LR - kItemBits);
   auto copy_group = [&](uint64_t gg) {
-    const int m = sh.pd.m, r = sh.pd.r;
-    const int T = 1 << (m - r);
-    if (gg < (1ull << sh.pd.ngbits) && (int)t < T)
-      prefetch_group<Real, false>(reinterpret_cast<C*>(smem_raw), psi, gbase_of(gg, sh.gtab), sh.base[t], sh.pv,
-                                  T, 1 << (m - kItemBits) >> (m - r), t);
+    if (gg < (1ull << sh.pd.ngbits)) {
+      uint64_t P[V];
+      uint32_t D[V];
+      ex.template copy_offsets<V>(P, D);
+      const uint64_t b = gbase_of(gg, sh.gtab) | sh.base[t];
+      const uint32_t d = swz<Real>(t << kItemBits) * (uint32_t)sizeof(C);
+#pragma unroll
+      for (int v = 0; v < V; ++v) cp_async16(smem_raw + (d ^ D[v]), psi + (b | P[v]));
+    }
     cp_async_commit();
   };
   const uint64_t ngroups = 1ull << sh.pd.ngbits;
