@@ -92,3 +92,40 @@ def test_empty_and_tiny():
     qc.h(0)
     _, plan = tile_circuit(qc, 4)
     assert len(plan) == 1 and plan[0].layout == [0]
+
+
+def _both(qc, nL):
+    out = []
+    for native in (False, True):
+        _, plan = tile_circuit(qc, nL, native=native)
+        out.append(_record(qc, plan))
+    return out
+
+
+@pytest.mark.parametrize("nL", [1, 2, 7, 8, 40])
+def test_native_tiler_edge_sizes(nL):
+    # nL = 1: every 2-qubit gate forces a tile; nL >= n: one tile; barriers (no unitary) included
+    from frontierlabproject_b200 import circuits as C
+    qc = C.random_layered(8, 6, 9)
+    qc.barrier()
+    qc.cx(7, 0)
+    py, nat = _both(qc, nL)
+    assert nat == py
+    if nL >= 8:
+        assert len(nat) == 1
+
+
+def test_native_tiler_multi_qubit_targets():
+    # a gate on three qubits (a barrier over three wires) goes through the same set logic
+    from frontierlabproject_b200.circuit import QuantumCircuit
+    qc = QuantumCircuit(6)
+    for q in range(6):
+        qc.h(q)
+    qc.barrier(0, 2, 4)
+    qc.cx(0, 5)
+    qc.cx(1, 3)
+    qc.barrier(1, 3, 5)
+    qc.rz(0.3, 2)
+    for nL in (2, 3, 4, 6):
+        py, nat = _both(qc, nL)
+        assert nat == py
