@@ -244,7 +244,8 @@ struct Scan {
 };
 
 uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candidates, uint64_t forced,
-                    int cap, int iters, int restarts = 0) {
+                    int cap, int iters, int restarts = 0,
+                    std::vector<std::pair<size_t, uint64_t>>* optima = nullptr) {
   uint64_t S = forced;
   // greedy seed in op order
   uint64_t blocked = 0;
@@ -283,6 +284,7 @@ uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candid
     return bx;
   };
   size_t best = climb(S);
+  if (optima) optima->push_back({best, S});
   // iterated local search: restart the climb from the best set with three random bit swaps
   // (a fixed xorshift sequence per call: plans are deterministic), keep strict improvements
   uint64_t rng = 0x9E3779B97F4A7C15ull ^ ((uint64_t)rem.size() * 0xBF58476D1CE4E5B9ull);
@@ -307,6 +309,7 @@ uint64_t choose_set(const Scan& sc, const std::vector<int>& rem, uint64_t candid
       T = (T & ~bit(a)) | bit(b);
     }
     const size_t c = climb(T);
+    if (optima) optima->push_back({c, T});
     if (c > best) { best = c; S = T; }
   }
   return S;
@@ -364,7 +367,44 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
   std::vector<int> rem(ops.size()), taken, rest;
   for (size_t i = 0; i < ops.size(); ++i) rem[i] = (int)i;
   while (!rem.empty()) {
-    uint64_t S = (m == n) ? all : choose_set(sc, rem, all, forced, m, cfg.hill_iters, cfg.hill_iters);
+    uint64_t S = all;
+    if (m < n) {
+      // lookahead: among the 4 best distinct local optima of the search, the set after which
+      // `lookahead` more greedy passes execute the most gates
+      std::vector<std::pair<size_t, uint64_t>> opt;
+      S = choose_set(sc, rem, all, forced, m, cfg.hill_iters, cfg.hill_iters, cfg.lookahead > 0 ? &opt : nullptr);
+      if (cfg.lookahead > 0 && opt.size() > 1) {
+        std::stable_sort(opt.begin(), opt.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        std::vector<std::pair<size_t, uint64_t>> cand;
+        for (const auto& o : opt) {
+          bool dup = false;
+          for (const auto& c : cand) dup = dup || c.second == o.second;
+          if (!dup) cand.push_back(o);
+          if (cand.size() == 4) break;
+        }
+        std::vector<int> r1, r2, tk;
+        auto drop = [&](const std::vector<int>& r, uint64_t X, std::vector<int>& out) {
+          sc.run(r, X, tk);
+          out.clear();
+          size_t t2 = 0;
+          for (int i : r) {
+            if (t2 < tk.size() && tk[t2] == i) { ++t2; continue; }
+            out.push_back(i);
+          }
+          return tk.size();
+        };
+        size_t best_v = 0;
+        for (const auto& c : cand) {
+          size_t v = drop(rem, c.second, r1);
+          for (int d = 0; d < cfg.lookahead && !r1.empty(); ++d) {
+            const uint64_t S2 = choose_set(sc, r1, all, forced, m, cfg.hill_iters, 4);
+            v += drop(r1, S2, r2);
+            r1.swap(r2);
+          }
+          if (v > best_v) { best_v = v; S = c.second; }
+        }
+      }
+    }
     sc.run(rem, S, taken);
     if (taken.empty()) throw std::runtime_error("planner: pass made no progress");
     PlannedPass ps;

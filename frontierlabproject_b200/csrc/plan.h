@@ -44,6 +44,7 @@ struct PlanConfig {
   int hill_iters = 16;    // hill-climbing rounds when choosing the staged / register sets (and
                           // restarts of the staged-set search)
   bool pair_bit = false;  // physical bit 0 is a register bit of every phase (packed kernels)
+  int lookahead = 2;      // staged-set choice: greedy passes looked ahead over the 4 best candidates
 };
 
 struct PlannedPhase {
