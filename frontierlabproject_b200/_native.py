@@ -77,6 +77,7 @@ _SIGS = {
     "qs_permute_scatter": [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p],
     "qs_plan_info": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), POINTER(c_int)],
     "qs_lqr_flat_tiling": [c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p],
+    "qs_fuse_ops": [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p],
     "qs_plan_emulate": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), c_void_p],
     "qs_perm_emulate": [c_int, c_int, c_void_p, POINTER(QsConfig), c_void_p, POINTER(c_int)],
     "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), c_void_p, c_int],

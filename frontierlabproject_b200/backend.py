@@ -131,12 +131,15 @@ def tile_ops_for(tile, qubit_map: dict, np_dtype) -> list:
 
 def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional[int] = None,
                        use_float32: bool = False, use_cuda_graphs: bool = True, tile_mode: str = "cooperative",
-                       enable_fusion: bool = True, logical_order: bool = False, sv=None, out: np.ndarray = None):
+                       enable_fusion: bool = True, logical_order: bool = False, sv=None, out: np.ndarray = None,
+                       native_fusion: bool = False):
     """Simulate ``qc`` along ``tile_plan``; returns (statevector ndarray, metrics).
 
     ``sv`` may be an existing Statevector/StatevectorF32 of the right size, reset to
     |0...0> here (avoids re-allocating HBM between runs); ``out`` an existing host array
-    (e.g. pinned) that receives the result.
+    (e.g. pinned) that receives the result; ``native_fusion`` packs each tile's ops and fuses
+    them in the native library (``qs_fuse_ops``, the same fusion) instead of the Python loop
+    (host matrices only; device matrices keep the Python path).
     """
     if tile_mode not in ("cooperative", "graphed", "sequential"):
         raise ValueError(f"unknown tile_mode: {tile_mode}")
@@ -168,7 +171,9 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
         ops = tile_ops_for(tile, qubit_map, np_dtype)
         num_gates += len(ops)
         if ops:
-            if enable_fusion:
+            if enable_fusion and native_fusion and all(isinstance(o[-1], np.ndarray) for o in ops):
+                ops = _OpBatch(ops, 0 if np_dtype == np.complex64 else 1).fused()
+            elif enable_fusion:
                 ops = fuse_tile_ops(ops)
             num_fused_ops += len(ops)
             if tile_mode == "cooperative":

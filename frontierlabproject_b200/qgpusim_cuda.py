@@ -52,6 +52,7 @@ class _OpBatch:
     def __init__(self, ops: Sequence, dtype_code: int):
         typestr, npdt = _TYPESTR[dtype_code]
         n = len(ops)
+        self._code = dtype_code
         self.arr = np.zeros(n, dtype=N.OP_DTYPE)
         self._keep: List[np.ndarray] = []
         kinds: List[int] = []
@@ -111,6 +112,20 @@ class _OpBatch:
             offs = np.cumsum(sizes) - sizes  # entry offset of each matrix in buf
             self.arr["U"][np.asarray(host_idx)] = np.uint64(buf.ctypes.data) + offs * np.uint64(item)
             self._keep.append(buf)
+
+    def fused(self) -> "_OpBatch":
+        """The ops fused natively (``qs_fuse_ops``: consecutive gates on the same qubit / ordered
+        pair multiplied, as ``backend.fuse_tile_ops``); host matrices only."""
+        out = _OpBatch.__new__(_OpBatch)
+        n = len(self.arr)
+        out.arr = np.zeros(n, dtype=N.OP_DTYPE)
+        mats = np.empty(16 * max(n, 1), dtype=np.complex64 if self._code == N.QS_C64 else np.complex128)
+        nout = c_int()
+        N.call("qs_fuse_ops", self._code, self.ptr, n, out.arr.ctypes.data, mats.ctypes.data, byref(nout))
+        out.arr = out.arr[:nout.value]
+        out._keep = [mats]
+        out._code = self._code
+        return out
 
     @property
     def ptr(self) -> int:

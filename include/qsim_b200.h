@@ -214,6 +214,13 @@ QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_o
 QS_API int qs_lqr_flat_tiling(int num_qubits, int nL, const unsigned long long* targets, int ngates, int* order,
                               int* tile_of, unsigned long long* tile_masks, int* ntiles);
 
+/* Gate fusion of a tile's op list on the host (replaces the Python loop of fuse_tile_ops,
+ * qgpusim/backends/custom/backend.py:88-200; same result: consecutive gates on the same qubit /
+ * the same ordered qubit pair multiplied, U_new = U @ U_prev).  in: nin ops with host matrices
+ * of dtype; out: room for nin ops, whose U point into mats (room for nin * 16 entries of
+ * dtype); *nout = fused count.  Device matrices are rejected (fuse those on the caller side). */
+QS_API int qs_fuse_ops(int dtype, const qs_op* in, int nin, qs_op* out, void* mats, int* nout);
+
 /* Planner inspection (host only, no GPU needed): plan the ops of a tile list for an
  * n-qubit state and report sweeps / phases.  ops use physical bits. */
 QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg,
