@@ -19,6 +19,9 @@ QS_C128 = 1
 MODES = {"cooperative": 0, "graphed": 1, "sequential": 2}
 QS_OP_1Q = 1
 QS_OP_2Q = 2
+QS_ERR_INVALID = -1
+QS_ERR_CUDA = -2
+QS_ERR_DEVICE = -3
 
 # qs_op {int kind, q0, q1, u_on_device; const void* U}
 OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
@@ -28,7 +31,7 @@ OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
 
 class QsConfig(ctypes.Structure):
     _fields_ = [("m", c_int), ("k", c_int), ("hill_iters", c_int), ("grid_mult", c_int), ("jit", c_int),
-                ("jit_lr", c_int), ("jit_blocks", c_int), ("jit_packed", c_int)]
+                ("jit_lr", c_int), ("jit_blocks", c_int), ("jit_packed", c_int), ("wait_limit_ns", c_ulonglong)]
 
 
 class QsStats(ctypes.Structure):
@@ -43,6 +46,7 @@ class QsStats(ctypes.Structure):
 # name -> (argtypes); every function returns int status
 _SIGS = {
     "qs_version": [],
+    "qs_debug_fail_alloc": [c_int],
     "qs_device_count": [POINTER(c_int)],
     "qs_create": [c_int, c_int, POINTER(c_void_p)],
     "qs_destroy": [c_void_p],

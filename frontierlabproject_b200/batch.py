@@ -6,7 +6,7 @@ fixed gates), its parameters and an observable H = sum_i a_i Z_i Z_{i+1} + b_i X
 instances (n <= ``small_max``) run wholly in shared memory; larger ones stream their states
 from an HBM arena in planned passes of 2^m staged amplitudes (``m``), ``chunk`` groups per
 work item.  ``autotune`` times candidate shapes on the batch itself and keeps the fastest
-(cached by the batch's size signature).
+(cached by the batch's size signature, in the process and in a JSON file).
 
 The device code is libqsim_b200's ``batch_kernel`` (C ABI ``qs_batch_*``); ``emulate`` runs
 the same program on the host (FP64) for tests.
@@ -15,6 +15,8 @@ from __future__ import annotations
 
 import ctypes
 import itertools
+import json
+import os
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -31,7 +33,8 @@ class QsBatchInstance(ctypes.Structure):
 
 class QsBatchConfig(ctypes.Structure):
     _fields_ = [("m", ctypes.c_int), ("small_max", ctypes.c_int), ("chunk", ctypes.c_int),
-                ("threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int)]
+                ("threads", ctypes.c_int), ("blocks_per_sm", ctypes.c_int), ("pad", ctypes.c_int),
+                ("wait_limit_ns", ctypes.c_ulonglong)]
 
 
 @dataclass
@@ -49,9 +52,11 @@ class BatchShape:
     chunk: int = 4
     threads: int = 256
     blocks_per_sm: int = 0
+    wait_limit_ns: int = 0   # dependency waits of the kernel (0: the library default, 10 s)
 
     def c(self) -> QsBatchConfig:
-        return QsBatchConfig(self.m, self.small_max, self.chunk, self.threads, self.blocks_per_sm)
+        return QsBatchConfig(self.m, self.small_max, self.chunk, self.threads, self.blocks_per_sm, 0,
+                             self.wait_limit_ns)
 
 
 def hea_batch(count: int, n_range=(12, 22), l_range=(4, 16), seed: int = 0) -> List[Instance]:
@@ -171,6 +176,51 @@ class BatchedAdjoint:
 _TUNED: Dict[tuple, BatchShape] = {}
 
 
+def autotune_cache_path() -> str:
+    """JSON file of tuned shapes: $QSIM_AUTOTUNE_CACHE, else ~/.cache/qsim_b200/autotune.json."""
+    p = os.environ.get("QSIM_AUTOTUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "qsim_b200", "autotune.json")
+
+
+def _device_tag() -> str:
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.get_device_name(torch.cuda.current_device())
+    except Exception:
+        pass
+    return "unknown-device"
+
+
+def _cache_key(sig: tuple) -> str:
+    return _device_tag() + "|" + json.dumps([[list(k), v] for k, v in sig])
+
+
+def _load_cache(path: str) -> Dict[str, dict]:
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d if isinstance(d, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_cache(path: str, key: str, shape: BatchShape) -> None:
+    d = _load_cache(path)
+    d[key] = {"m": shape.m, "small_max": shape.small_max, "chunk": shape.chunk, "threads": shape.threads,
+              "blocks_per_sm": shape.blocks_per_sm}
+    try:
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        tmp = path + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass  # an unwritable cache only costs a re-tune in the next process
+
+
 def _signature(insts: Sequence[Instance]) -> tuple:
     """Size signature of a batch: count of instances per (qubits, gates) bucket."""
     hist: Dict[tuple, int] = {}
@@ -190,12 +240,27 @@ def candidate_shapes(max_qubits: int) -> List[BatchShape]:
 
 
 def autotune(insts: Sequence[Instance], shapes: Optional[Sequence[BatchShape]] = None, reps: int = 2,
-             verbose: bool = False) -> BatchShape:
+             verbose: bool = False, cache_path: Optional[str] = None, persist: bool = True) -> BatchShape:
     """Time each candidate shape on this batch (device time of the launch, best of ``reps``)
-    and return the fastest; results are cached by the batch's size signature."""
+    and return the fastest.  Results are cached by the batch's size signature and the device
+    name, in this process and (``persist``) in the JSON file ``cache_path`` (default
+    ``autotune_cache_path()``), so a later process with a batch of the same sizes skips the
+    timing runs."""
     sig = _signature(insts)
     if sig in _TUNED:
         return _TUNED[sig]
+    path = cache_path or autotune_cache_path()
+    key = _cache_key(sig)
+    if persist:
+        hit = _load_cache(path).get(key)
+        if hit is not None:
+            try:
+                shape = BatchShape(**{k: int(hit[k]) for k in ("m", "small_max", "chunk", "threads",
+                                                                "blocks_per_sm")})
+                _TUNED[sig] = shape
+                return shape
+            except (KeyError, TypeError, ValueError):
+                pass
     nmax = max(inst.circuit.num_qubits for inst in insts)
     best, best_ms = None, float("inf")
     for shape in (shapes or candidate_shapes(nmax)):
@@ -214,4 +279,6 @@ def autotune(insts: Sequence[Instance], shapes: Optional[Sequence[BatchShape]] =
     if best is None:
         raise RuntimeError("autotune: no candidate shape runs this batch")
     _TUNED[sig] = best
+    if persist:
+        _store_cache(path, key, best)
     return best

@@ -50,12 +50,14 @@ constexpr uint64_t kBatchWaitNs = 10ull * 1000ull * 1000ull * 1000ull;  // 10 s 
 
 struct Cfg {
   int m = 13, small_max = 13, chunk = 4, threads = 256, bps = 0;
+  uint64_t wait_ns = kBatchWaitNs;
 };
 
 Cfg cfg_of(const qs_batch_config* c) {
   Cfg k;
   if (c) {
     k.m = c->m; k.small_max = c->small_max; k.chunk = c->chunk; k.threads = c->threads; k.bps = c->blocks_per_sm;
+    if (c->wait_limit_ns) k.wait_ns = c->wait_limit_ns;
   }
   if (k.m < 9 || k.m > kBatchMaxLocal) bad("batch: m must be in 9..13");
   if (k.small_max < 0 || k.small_max > kBatchMaxLocal) bad("batch: small_max must be in 0..13");
@@ -587,11 +589,11 @@ int qs_batch_create(const qs_batch_instance* insts, int ninst, const qs_batch_co
     b->cfg = c;
     for (auto& x : in) { b->n.push_back(x.n); b->nparam.push_back(x.nparam); }
     b->enc = encode_batch(in, c, &b->plans);
-    BCK(cudaMalloc(&b->d_prog, b->enc.bytes.size()));
+    BCK(dev_malloc((void**)&b->d_prog, b->enc.bytes.size()));
     BCK(cudaMemcpy(b->d_prog, b->enc.bytes.data(), b->enc.bytes.size(), cudaMemcpyHostToDevice));
-    if (b->enc.arena_amps) BCK(cudaMalloc(&b->d_arena, b->enc.arena_amps * sizeof(float2)));
-    BCK(cudaMalloc(&b->d_grads, (b->enc.nparam_total + ninst) * sizeof(double)));
-    BCK(cudaMalloc(&b->d_ctl, (2 + ninst) * sizeof(unsigned)));
+    if (b->enc.arena_amps) BCK(dev_malloc(&b->d_arena, b->enc.arena_amps * sizeof(float2)));
+    BCK(dev_malloc((void**)&b->d_grads, (b->enc.nparam_total + ninst) * sizeof(double)));
+    BCK(dev_malloc((void**)&b->d_ctl, (2 + ninst) * sizeof(unsigned)));
     BCK(cudaEventCreate(&b->ev0));
     BCK(cudaEventCreate(&b->ev1));
     *out = b.release();
@@ -612,7 +614,7 @@ int qs_batch_set_params(qs_batch* b, const qs_batch_instance* insts, int ninst) 
     if (e.bytes.size() > b->enc.bytes.size()) {
       BCK(cudaFree(b->d_prog));
       b->d_prog = nullptr;
-      BCK(cudaMalloc(&b->d_prog, e.bytes.size()));
+      BCK(dev_malloc((void**)&b->d_prog, e.bytes.size()));
     }
     b->enc = std::move(e);
     BCK(cudaMemcpy(b->d_prog, b->enc.bytes.data(), b->enc.bytes.size(), cudaMemcpyHostToDevice));
@@ -628,7 +630,7 @@ int qs_batch_run(qs_batch* b, void* stream, float* ms) {
     BCK(cudaMemsetAsync(b->d_ctl, 0, (2 + ninst) * sizeof(unsigned), s));
     BCK(cudaEventRecord(b->ev0, s));
     BCK(launch_batch(b->d_prog, b->d_arena, b->d_grads, b->d_grads + b->enc.nparam_total, b->d_ctl,
-                     b->cfg.threads, b->enc.mbuf, b->cfg.bps, kBatchWaitNs, s, &b->grid));
+                     b->cfg.threads, b->enc.mbuf, b->cfg.bps, b->cfg.wait_ns, s, &b->grid));
     BCK(cudaEventRecord(b->ev1, s));
     if (ms) {
       BCK(cudaEventSynchronize(b->ev1));

@@ -142,14 +142,15 @@ __global__ void norm2_kernel(const C* __restrict__ psi, int n, double* acc) {
   }
 }
 
-// <a|b> = sum conj(a) b
-template <typename C>
-__global__ void inner_kernel(const C* __restrict__ a, const C* __restrict__ b, int n, double* acc) {
+// <a|b> = sum conj(a) b (a and b may differ in precision: complex64 against complex128)
+template <typename CA, typename CB>
+__global__ void inner_kernel(const CA* __restrict__ a, const CB* __restrict__ b, int n, double* acc) {
   __shared__ double pr[32], pi[32];
   const uint64_t dim = 1ull << n;
   double sr = 0.0, si = 0.0;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
-    const C x = a[i], y = b[i];
+    const CA x = a[i];
+    const CB y = b[i];
     sr += (double)x.x * y.x + (double)x.y * y.y;
     si += (double)x.x * y.y - (double)x.y * y.x;
   }
@@ -234,10 +235,21 @@ cudaError_t launch_norm2(int dtype, const void* psi, int n, double* acc, cudaStr
 }
 
 cudaError_t launch_inner(int dtype, const void* a, const void* b, int n, double* acc2, cudaStream_t s) {
+  return launch_inner_mixed(dtype, a, dtype, b, n, acc2, s);
+}
+
+cudaError_t launch_inner_mixed(int dtype_a, const void* a, int dtype_b, const void* b, int n, double* acc2,
+                               cudaStream_t s) {
   const int th = 512;
   const int grid = grid_for(1ull << n, th);
-  if (dtype == 0) inner_kernel<float2><<<grid, th, 0, s>>>((const float2*)a, (const float2*)b, n, acc2);
-  else inner_kernel<double2><<<grid, th, 0, s>>>((const double2*)a, (const double2*)b, n, acc2);
+  if (dtype_a == 0 && dtype_b == 0)
+    inner_kernel<float2, float2><<<grid, th, 0, s>>>((const float2*)a, (const float2*)b, n, acc2);
+  else if (dtype_a == 0)
+    inner_kernel<float2, double2><<<grid, th, 0, s>>>((const float2*)a, (const double2*)b, n, acc2);
+  else if (dtype_b == 0)
+    inner_kernel<double2, float2><<<grid, th, 0, s>>>((const double2*)a, (const float2*)b, n, acc2);
+  else
+    inner_kernel<double2, double2><<<grid, th, 0, s>>>((const double2*)a, (const double2*)b, n, acc2);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/qsim_b200.h"
+#include "abi_ops.h"
 #include "kernels.h"
 #include "pass_body.cuh"
 #include "plan.h"
@@ -414,69 +415,53 @@ cudaError_t launch_ws(const uint8_t* prog, void* psi, int npass, int threads, si
 extern "C" QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_op* ops, int nops,
                                           void* stream) {
   using namespace qsb;
+  const char* kWho = "qs_apply_ops_noalloc";
   auto fail = [&](const std::string& m) {
     set_last_error(m);
     return QS_ERR_INVALID;
   };
   auto cuda_fail = [&](cudaError_t e) {
-    fail(std::string("CUDA error: ") + cudaGetErrorString(e));
+    set_last_error(std::string("CUDA error: ") + cudaGetErrorString(e));
     return QS_ERR_CUDA;
   };
-  if (!psi || (nops > 0 && !ops)) return fail("qs_apply_ops_noalloc: null argument");
-  if (dtype != QS_C64 && dtype != QS_C128) return fail("qs_apply_ops_noalloc: dtype must be QS_C64 or QS_C128");
+  if (!psi || (nops > 0 && !ops)) return fail(std::string(kWho) + ": null argument");
+  if (dtype != QS_C64 && dtype != QS_C128) return fail(std::string(kWho) + ": dtype must be QS_C64 or QS_C128");
+  // the sweep kernel moves the state in 16-byte units
+  if (reinterpret_cast<uintptr_t>(psi) & 15u)
+    return fail(std::string(kWho) + ": psi must be 16-byte aligned");
   const int r = dtype == 0 ? 5 : 4;
   if (num_qubits < r + 1 || num_qubits > 36)
-    return fail("qs_apply_ops_noalloc: num_qubits must be in [" + std::to_string(r + 1) + ", 36]");
+    return fail(std::string(kWho) + ": num_qubits must be in [" + std::to_string(r + 1) + ", 36]");
+  if (nops < 0) return fail(std::string(kWho) + ": invalid op list");
   if (nops == 0) return 0;
-  std::vector<QOp> q;
   try {
-    q.reserve(nops);
-    const size_t esz = dtype == 0 ? 8 : 16;
-    for (int i = 0; i < nops; ++i) {
-      const qs_op& o = ops[i];
-      QOp x;
-      int cnt = 0;
-      if (o.kind == QS_OP_1Q) {
-        if (o.q0 < 0 || o.q0 >= num_qubits) return fail("apply_tile_dev: invalid q0");
-        x.arity = 1; x.q0 = o.q0; cnt = 4;
-      } else if (o.kind == QS_OP_2Q) {
-        if (o.q0 < 0 || o.q0 >= num_qubits || o.q1 < 0 || o.q1 >= num_qubits)
-          return fail("apply_tile_dev: invalid q0/q1");
-        if (o.q0 == o.q1) return fail("apply_tile_dev: q0 == q1");
-        x.arity = 2; x.q0 = o.q0; x.q1 = o.q1; cnt = 16;
-      } else {
-        return fail("apply_tile_dev: unknown op kind: " + std::to_string(o.kind));
-      }
-      if (!o.U) return fail("apply_tile_dev: null gate matrix");
-      if (o.u_on_device) return fail("qs_apply_ops_noalloc: gate matrices must be host memory");
-      for (int k = 0; k < cnt; ++k) {
-        if (esz == 8) {
-          const float* f = static_cast<const float*>(o.U);
-          x.U[k] = cplx(f[2 * k], f[2 * k + 1]);
-        } else {
-          const double* f = static_cast<const double*>(o.U);
-          x.U[k] = cplx(f[2 * k], f[2 * k + 1]);
-        }
-      }
-      q.push_back(x);
+    // psi must be device (or managed) memory that the current device can address
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e);
+    cudaPointerAttributes attr{};
+    e = cudaPointerGetAttributes(&attr, psi);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(std::string(kWho) + ": psi is not a device pointer");
     }
+    if (!(attr.type == cudaMemoryTypeManaged || (attr.type == cudaMemoryTypeDevice && attr.device == dev)))
+      return fail(std::string(kWho) + ": psi must be device memory of the current device");
+    std::vector<QOp> q = convert_abi_ops(ops, nops, num_qubits, dtype, kWho, nullptr, false);
     std::vector<COp> cops;
+    cops.reserve(q.size());
     for (const QOp& o : q) cops.push_back(classify(o));
     PlanConfig pc;
     pc.r = r;
     pc.m = std::max(r, std::min(dtype == 0 ? 13 : 12, num_qubits));
-    auto passes = plan_passes(cops, num_qubits, pc);
-    for (const PlannedPass& ps : passes) extract_pass_scalars(q, ps.ops);
-    cops.clear();
-    for (const QOp& o : q) cops.push_back(classify(o));
-    Program prog = encode_program(passes, cops, num_qubits, dtype, r);
+    const auto passes = plan_passes(cops, num_qubits, pc);
+    const Program prog = build_program(q, passes, num_qubits, dtype, r);
     if (prog.bytes.size() > kWorkspaceBytes - kWorkspaceCtl)
-      return fail("qs_apply_ops_noalloc: the program of these ops needs " + std::to_string(prog.bytes.size()) +
+      return fail(std::string(kWho) + ": the program of these ops needs " + std::to_string(prog.bytes.size()) +
                   " bytes; the static workspace holds " + std::to_string(kWorkspaceBytes - kWorkspaceCtl) +
                   " (split the ops into smaller calls)");
     unsigned char* ws = nullptr;
-    cudaError_t e = workspace_address(&ws);
-    if (e != cudaSuccess) return cuda_fail(e);
+    if ((e = workspace_address(&ws)) != cudaSuccess) return cuda_fail(e);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned* ctl = reinterpret_cast<unsigned*>(ws);
     // the barrier and error words must start at zero for every call
@@ -484,22 +469,24 @@ extern "C" QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits,
     if ((e = cudaMemcpyAsync(ws + kWorkspaceCtl, prog.bytes.data(), prog.bytes.size(), cudaMemcpyHostToDevice, s)) !=
         cudaSuccess)
       return cuda_fail(e);
-    const uint64_t limit = 20ull * 1000 * 1000 * 1000;
     e = dtype == 0 ? launch_ws<float, 5>(ws + kWorkspaceCtl, psi, prog.npass, prog.threads, prog.max_smem, ctl,
-                                          ctl + 2, limit, s)
+                                          ctl + 2, kDeviceWaitLimitNs, s)
                    : launch_ws<double, 4>(ws + kWorkspaceCtl, psi, prog.npass, prog.threads, prog.max_smem, ctl,
-                                           ctl + 2, limit, s);
+                                           ctl + 2, kDeviceWaitLimitNs, s);
     if (e != cudaSuccess) return cuda_fail(e);
     unsigned word = 0;
     if ((e = cudaMemcpyAsync(&word, ctl + 2, sizeof(word), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return cuda_fail(e);
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e);
     if (word != 0) {
-      fail("qs_apply_ops_noalloc: device error: a grid barrier wait expired");
+      set_last_error(std::string(kWho) + ": device error: " + device_error_name(word) + " (error word " +
+                     std::to_string(word) + ")");
       return QS_ERR_DEVICE;
     }
   } catch (const std::exception& ex) {
     return fail(ex.what());
+  } catch (...) {
+    return fail(std::string(kWho) + ": unexpected error");
   }
   return 0;
 }

@@ -25,6 +25,8 @@ cudaError_t launch_permute_scatter(int dtype, const void* in, void* out, int n, 
 // reductions into double accumulators (kern_gate.cu); acc must be zeroed by the caller
 cudaError_t launch_norm2(int dtype, const void* psi, int n, double* acc, cudaStream_t s);
 cudaError_t launch_inner(int dtype, const void* a, const void* b, int n, double* acc2, cudaStream_t s);
+cudaError_t launch_inner_mixed(int dtype_a, const void* a, int dtype_b, const void* b, int n, double* acc2,
+                               cudaStream_t s);
 cudaError_t launch_set_basis(int dtype, void* psi, int n, uint64_t index, cudaStream_t s);
 
 // adjoint differentiation (kern_adjoint.cu)
@@ -54,6 +56,27 @@ cudaError_t launch_sample(int dtype, const void* psi, int n, uint64_t shots, uin
                           uint64_t* out, cudaStream_t s);
 
 int device_sm_count();
+
+// Every device / pinned-host allocation of the library goes through these.  After
+// qs_debug_fail_alloc(k), the k-th next one fails with cudaErrorMemoryAllocation and
+// allocates nothing, so tests can check that each error path releases what it holds.
+cudaError_t dev_malloc(void** p, size_t bytes);
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t s);
+cudaError_t host_malloc(void** p, size_t bytes);
+
+// Device buffer from the stream-ordered allocator, freed in stream order when it goes out of
+// scope (also when an exception leaves the scope).
+struct AsyncBuf {
+  void* p = nullptr;
+  cudaStream_t s = nullptr;
+  explicit AsyncBuf(cudaStream_t st) : s(st) {}
+  AsyncBuf(const AsyncBuf&) = delete;
+  AsyncBuf& operator=(const AsyncBuf&) = delete;
+  cudaError_t alloc(size_t bytes) { return dev_malloc_async(&p, bytes, s); }
+  ~AsyncBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
 
 // message returned by qs_last_error() on the calling thread (state.cu)
 void set_last_error(const std::string& msg);

@@ -2,6 +2,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 
@@ -158,9 +159,24 @@ bool same_shape(const QOp& o, const cplx* V) {
 
 }  // namespace
 
+Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& passes, int n, int dtype, int r) {
+  for (const PlannedPass& ps : passes) extract_pass_scalars(ops, ps.ops);
+  std::vector<COp> cops;
+  cops.reserve(ops.size());
+  for (const QOp& o : ops) cops.push_back(classify(o));
+  return encode_program(passes, cops, n, dtype, r);
+}
+
 void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops) {
   cplx total(1.0, 0.0);
   int absorber = -1, absorber_cost = -1;
+  // Dividing a gate by its pivot p scales the state by 1/|p| until the pass's scalar is
+  // multiplied back in.  log2 of that running factor is kept within +-kMaxLog2 at every gate
+  // (whichever gate absorbs the product, the state stays within 2^(+-2 kMaxLog2) of its
+  // norm: far inside the single-precision exponent range); a gate whose pivot would leave
+  // the band keeps its matrix.
+  constexpr double kMaxLog2 = 24.0;
+  double log2_scale = 0.0;
   for (int oi : pass_ops) {
     QOp& o = ops[oi];
     const int d = o.arity == 1 ? 2 : 4;
@@ -170,23 +186,33 @@ void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_op
     if (scale == 0.0) continue;
     int best = matrix_cost(o.U, d);
     int best_e = -1;
+    double best_mag = 0.0;
     cplx bestV[16];
     for (int e = 0; e < d * d; ++e) {
-      if (std::abs(o.U[e]) < 1e-6 * scale) continue;  // keep scaled entries bounded
+      const double mag = std::abs(o.U[e]);
+      if (mag < 1e-6 * scale) continue;  // keep scaled entries bounded
+      const double step = -std::log2(mag);
+      if (std::abs(log2_scale + step) > kMaxLog2) continue;
       cplx V[16];
-      for (int k = 0; k < d * d; ++k) V[k] = snap(o.U[k] / o.U[e], scale / std::abs(o.U[e]));
+      for (int k = 0; k < d * d; ++k) V[k] = snap(o.U[k] / o.U[e], scale / mag);
       for (int k = 0; k < d * d; ++k)  // entries equal to the pivot divide to exactly one
         if (o.U[k] == o.U[e]) V[k] = cplx(1.0, 0.0);
       V[e] = cplx(1.0, 0.0);
       const int c = matrix_cost(V, d);
-      if (c < best && same_shape(o, V)) {
+      // among pivots of equal cost the first, unless a later one is far larger (RX(t) within
+      // about 0.008 of t = pi pivots on its sine, not on its vanishing cosine); the choice, and
+      // with it the zero/one/real/imaginary class of every entry, stays the same for most
+      // parameter values, so the specialised kernels are reused across parameter changes
+      if ((c < best || (c == best && best_e >= 0 && mag > 256.0 * best_mag)) && same_shape(o, V)) {
         best = c;
         best_e = e;
+        best_mag = mag;
         for (int k = 0; k < d * d; ++k) bestV[k] = V[k];
       }
     }
     if (best_e >= 0) {
       total *= o.U[best_e];
+      log2_scale -= std::log2(best_mag);
       for (int k = 0; k < d * d; ++k) o.U[k] = bestV[k];
     }
     // absorber: a gate whose shape survives scaling, and whose cost grows least

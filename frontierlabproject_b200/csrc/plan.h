@@ -86,6 +86,10 @@ struct Program {
 Program encode_program(const std::vector<PlannedPass>& passes, const std::vector<COp>& ops,
                        int n, int dtype, int r_req = 0);
 
+// The per-pass scalar extraction of ops (which keeps every gate's planned shape, so the plan
+// made from the original gates stays valid), then the encoded program of the passes.
+Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& passes, int n, int dtype, int r);
+
 // Reference interpretation of a program on host memory (used by CPU tests of the planner).
 void emulate_program(const uint8_t* prog, void* state, int n, int dtype);
 

@@ -101,6 +101,17 @@ enum DeviceError : uint32_t {
   DERR_LOAD_TIMEOUT = 3,   // a team's wait for its group copies expired (pass kernel, two teams)
 };
 
+#ifndef __CUDACC_RTC__
+inline const char* device_error_name(uint32_t w) {
+  switch (w) {
+    case DERR_BARRIER_TIMEOUT: return "a grid barrier wait expired";
+    case DERR_BAD_PROGRAM: return "the device program was rejected by the kernel";
+    case DERR_LOAD_TIMEOUT: return "a wait for group copies expired";
+    default: return "a bounded device wait expired";
+  }
+}
+#endif
+
 // Bank-spreading swizzle of a local amplitude index inside the shared-memory group.
 // complex64: XOR bits 1..3 with a fold of bits 4.. (bit 0 kept so aligned pairs stay together);
 // complex128: XOR bits 0..2 with a fold of bits 3..  Both are XOR-linear, so

@@ -10,10 +10,12 @@
 //  * Observation first moves the data to the current layout with in-place permutation
 //    passes (bit-exact), so pos2bit becomes the identity.
 #include <algorithm>
+#include <atomic>
 #include <complex>
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -21,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/qsim_b200.h"
+#include "abi_ops.h"
 #include "kernels.h"
 #include "jit.h"
 #include "plan.h"
@@ -51,6 +54,11 @@ struct InvalidArg {
   std::string msg;
 };
 
+// a kernel reported an error word (QS_ERR_DEVICE); the state stays usable
+struct DeviceFault {
+  std::string msg;
+};
+
 constexpr uint64_t kBarrierLimitNs = kDeviceWaitLimitNs;
 
 int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
@@ -59,21 +67,31 @@ int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
 
 namespace qsb {
 void set_last_error(const std::string& msg) { g_err = msg; }
-}  // namespace qsb
 
-namespace {
+// allocation fault injection: 0 = off, k > 0 = the k-th next allocation fails
+static std::atomic<long long> g_fail_alloc{0};
 
-// Encode the planned passes after the per-pass scalar extraction (which keeps every gate's
-// planned shape, so the plan made from the original gates stays valid).
-Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& passes, int n, int dtype, int r) {
-  for (const PlannedPass& ps : passes) extract_pass_scalars(ops, ps.ops);
-  std::vector<COp> cops;
-  cops.reserve(ops.size());
-  for (const QOp& o : ops) cops.push_back(classify(o));
-  return encode_program(passes, cops, n, dtype, r);
+static bool inject_alloc_failure() {
+  long long c = g_fail_alloc.load();
+  while (c > 0 && !g_fail_alloc.compare_exchange_weak(c, c - 1)) {
+  }
+  return c == 1;
 }
 
-}  // namespace
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMalloc(p, bytes);
+}
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t s) {
+  if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMallocAsync(p, bytes, s);
+}
+cudaError_t host_malloc(void** p, size_t bytes) {
+  if (inject_alloc_failure()) return cudaErrorMemoryAllocation;
+  return cudaMallocHost(p, bytes);
+}
+}  // namespace qsb
+
 
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
@@ -111,6 +129,8 @@ struct qs_state {
   int jit_packed = 0;      // FP32x2 arithmetic in the specialised kernels
   int jit_blocks = 2;      // resident blocks per SM of the specialised kernels (single-buffered
                            // blocks that overlap each other's group loads)
+  uint64_t wait_limit_ns = kBarrierLimitNs;  // bounded device waits of the pass kernel's grid
+                                             // barriers and the tensor-core kernel
   // device scratch: program buffer, control words (barrier x2, error), accumulators
   uint8_t* d_prog = nullptr;
   size_t prog_cap = 0;
@@ -154,8 +174,11 @@ struct qs_state {
     if (bytes > prog_cap) {
       CK(cudaStreamSynchronize(stream));
       if (d_prog) CK(cudaFree(d_prog));
-      prog_cap = std::max<size_t>(bytes * 2, 1 << 16);
-      CK(cudaMalloc(&d_prog, prog_cap));
+      d_prog = nullptr;
+      prog_cap = 0;
+      const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
+      CK(dev_malloc((void**)&d_prog, cap));
+      prog_cap = cap;
       if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
     }
   }
@@ -172,8 +195,11 @@ struct qs_state {
     CK(cudaEventSynchronize(s.done));  // the copy that last used this slot has run
     if (bytes > s.cap) {
       if (s.host) CK(cudaFreeHost(s.host));
-      s.cap = std::max<size_t>(bytes * 2, 1 << 16);
-      CK(cudaMallocHost(&s.host, s.cap));
+      s.host = nullptr;
+      s.cap = 0;
+      const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
+      CK(host_malloc((void**)&s.host, cap));
+      s.cap = cap;
     }
     std::memcpy(s.host, prog.bytes.data(), bytes);
     CK(cudaMemcpyAsync(d_prog, s.host, bytes, cudaMemcpyHostToDevice, stream));
@@ -205,7 +231,7 @@ struct qs_state {
     if (mode == QS_MODE_COOPERATIVE) {
       CK(cudaMemsetAsync(d_ctl, 0, 2 * sizeof(unsigned), stream));
       CK(launch_pass_kernel(dtype, d_prog, psi, 0, prog.npass, prog.threads, prog.max_smem, grid, true, d_ctl,
-                            d_ctl + 2, kBarrierLimitNs, stream));
+                            d_ctl + 2, wait_limit_ns, stream));
       st.launches += 1;
     } else {
       // specialised kernels for large complex64 states (compiled once per structure)
@@ -233,7 +259,7 @@ struct qs_state {
           e = jk ? jit_launch(*jk, p, d_prog, host_coef, psi, d_ctl + 2, prog.threads, prog.max_smem,
                               device_sm_count(), stream)
                  : launch_pass_kernel(dtype, d_prog, psi, p, p + 1, prog.threads, prog.max_smem, grid, false,
-                                      d_ctl, d_ctl + 2, kBarrierLimitNs, stream);
+                                      d_ctl, d_ctl + 2, wait_limit_ns, stream);
         cudaError_t e2 = cudaStreamEndCapture(stream, &g);
         if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
         if (e2 != cudaSuccess) throw CudaError{e2};
@@ -340,11 +366,10 @@ struct qs_state {
     for (int p = 0; p < n; ++p) perm[pos2bit[p]] = p;
     if (!use_pass_kernel()) {
       // tiny states: out-of-place scatter through a temporary buffer
-      void* tmp = nullptr;
-      CK(cudaMallocAsync(&tmp, dim * esz, stream));
-      CK(launch_permute_scatter(dtype, psi, tmp, n, perm.data(), stream));
-      CK(cudaMemcpyAsync(psi, tmp, dim * esz, cudaMemcpyDeviceToDevice, stream));
-      CK(cudaFreeAsync(tmp, stream));
+      AsyncBuf tmp(stream);
+      CK(tmp.alloc(dim * esz));
+      CK(launch_permute_scatter(dtype, psi, tmp.p, n, perm.data(), stream));
+      CK(cudaMemcpyAsync(psi, tmp.p, dim * esz, cudaMemcpyDeviceToDevice, stream));
       st.launches += 1;
     } else {
       PlanConfig c = eff_cfg();
@@ -363,7 +388,9 @@ struct qs_state {
     CK(cudaStreamSynchronize(stream));
     if (w[2] != 0) {
       CK(cudaMemsetAsync(d_ctl, 0, 3 * sizeof(unsigned), stream));
-      throw InvalidArg{"device error: a bounded device wait expired (error word " + std::to_string(w[2]) + ")"};
+      CK(cudaStreamSynchronize(stream));
+      throw DeviceFault{"device error: " + std::string(device_error_name(w[2])) + " (error word " +
+                        std::to_string(w[2]) + ")"};
     }
   }
 
@@ -386,6 +413,8 @@ int guard(F&& f) {
     return 0;
   } catch (const InvalidArg& e) {
     return fail(QS_ERR_INVALID, e.msg);
+  } catch (const DeviceFault& e) {
+    return fail(QS_ERR_DEVICE, e.msg);
   } catch (const CudaError& e) {
     return fail(QS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e.e));
   } catch (const std::exception& e) {
@@ -411,33 +440,49 @@ void read_matrix(const qs_state* s, int dtype, const void* U, int u_on_device, i
   (void)s;
 }
 
-// validate a tile op list like parse_tile_ops (bindings.cpp:182-220) and convert it
-std::vector<QOp> convert_ops(const qs_state* s, const qs_op* ops, int nops, int n, int dtype, bool map_layout) {
+}  // namespace
+
+namespace qsb {
+
+std::vector<QOp> convert_abi_ops(const qs_op* ops, int nops, int n, int dtype, const char* who, const int* pos2bit,
+                                 bool allow_device) {
+  const std::string w(who);
   std::vector<QOp> out;
-  out.reserve(nops);
+  out.reserve(nops > 0 ? nops : 0);
   for (int i = 0; i < nops; ++i) {
     const qs_op& o = ops[i];
     QOp q;
+    int count = 0;
     if (o.kind == QS_OP_1Q) {
-      if (o.q0 < 0 || o.q0 >= n) throw InvalidArg{"apply_tile_dev: invalid q0"};
-      if (!o.U) throw InvalidArg{"apply_tile_dev: null gate matrix"};
+      if (o.q0 < 0 || o.q0 >= n) throw std::invalid_argument(w + ": invalid q0");
       q.arity = 1;
-      q.q0 = map_layout ? s->pos2bit[o.q0] : o.q0;
-      read_matrix(s, dtype, o.U, o.u_on_device, 4, q.U);
+      q.q0 = pos2bit ? pos2bit[o.q0] : o.q0;
+      count = 4;
     } else if (o.kind == QS_OP_2Q) {
-      if (o.q0 < 0 || o.q0 >= n || o.q1 < 0 || o.q1 >= n) throw InvalidArg{"apply_tile_dev: invalid q0/q1"};
-      if (o.q0 == o.q1) throw InvalidArg{"apply_tile_dev: q0 == q1"};
-      if (!o.U) throw InvalidArg{"apply_tile_dev: null gate matrix"};
+      if (o.q0 < 0 || o.q0 >= n || o.q1 < 0 || o.q1 >= n) throw std::invalid_argument(w + ": invalid q0/q1");
+      if (o.q0 == o.q1) throw std::invalid_argument(w + ": q0 == q1");
       q.arity = 2;
-      q.q0 = map_layout ? s->pos2bit[o.q0] : o.q0;
-      q.q1 = map_layout ? s->pos2bit[o.q1] : o.q1;
-      read_matrix(s, dtype, o.U, o.u_on_device, 16, q.U);
+      q.q0 = pos2bit ? pos2bit[o.q0] : o.q0;
+      q.q1 = pos2bit ? pos2bit[o.q1] : o.q1;
+      count = 16;
     } else {
-      throw InvalidArg{"apply_tile_dev: unknown op kind: " + std::to_string(o.kind)};
+      throw std::invalid_argument(w + ": unknown op kind: " + std::to_string(o.kind));
     }
+    if (!o.U) throw std::invalid_argument(w + ": null gate matrix");
+    if (o.u_on_device && !allow_device) throw std::invalid_argument(w + ": gate matrices must be host memory");
+    read_matrix(nullptr, dtype, o.U, o.u_on_device, count, q.U);
     out.push_back(q);
   }
   return out;
+}
+
+}  // namespace qsb
+
+namespace {
+
+// the tile API's op list (validated as apply_tile_dev), at physical bits when map_layout
+std::vector<QOp> convert_ops(const qs_state* s, const qs_op* ops, int nops, int n, int dtype, bool map_layout) {
+  return convert_abi_ops(ops, nops, n, dtype, "apply_tile_dev", map_layout ? s->pos2bit.data() : nullptr, true);
 }
 
 void enqueue(qs_state* s, std::vector<QOp>&& ops, int mode) {
@@ -462,6 +507,11 @@ void enqueue(qs_state* s, std::vector<QOp>&& ops, int mode) {
 extern "C" {
 
 const char* qs_last_error(void) { return g_err.c_str(); }
+
+int qs_debug_fail_alloc(int k) {
+  g_fail_alloc.store(k > 0 ? k : 0);
+  return 0;
+}
 int qs_version(void) { return 100; }
 
 int qs_device_count(int* out) {
@@ -489,10 +539,10 @@ int qs_create(int num_qubits, int dtype, qs_state** out) {
     s->pos2bit.resize(num_qubits);
     for (int p = 0; p < num_qubits; ++p) s->pos2bit[p] = p;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    CK(cudaMalloc(&s->psi, s->dim * s->esz));
-    CK(cudaMalloc(&s->d_ctl, 4 * sizeof(unsigned)));
-    CK(cudaMalloc(&s->d_acc, 8 * sizeof(double)));
-    CK(cudaMallocHost(&s->h_acc, 8 * sizeof(double)));
+    CK(dev_malloc(&s->psi, s->dim * s->esz));
+    CK(dev_malloc((void**)&s->d_ctl, 4 * sizeof(unsigned)));
+    CK(dev_malloc((void**)&s->d_acc, 8 * sizeof(double)));
+    CK(host_malloc((void**)&s->h_acc, 8 * sizeof(double)));
     CK(cudaMemsetAsync(s->d_ctl, 0, 4 * sizeof(unsigned), s->stream));
     CK(launch_set_basis(dtype, s->psi, num_qubits, 0, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -640,14 +690,11 @@ int qs_sample(qs_state* s, unsigned long long shots, unsigned long long seed, un
     if (shots == 0) return;
     if (shots > (1ull << 31)) throw InvalidArg{"sample: at most 2^31 shots per call"};
     s->materialize();  // indices are layout (logical) indices
-    void* scratch = nullptr;
-    uint64_t* d_out = nullptr;
-    CK(cudaMallocAsync(&scratch, sample_scratch_bytes(s->n, shots), s->stream));
-    CK(cudaMallocAsync((void**)&d_out, shots * sizeof(uint64_t), s->stream));
-    CK(launch_sample(s->dtype, s->psi, s->n, shots, seed, scratch, d_out, s->stream));
-    CK(cudaMemcpyAsync(out, d_out, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
-    CK(cudaFreeAsync(scratch, s->stream));
-    CK(cudaFreeAsync(d_out, s->stream));
+    AsyncBuf scratch(s->stream), d_out(s->stream);
+    CK(scratch.alloc(sample_scratch_bytes(s->n, shots)));
+    CK(d_out.alloc(shots * sizeof(uint64_t)));
+    CK(launch_sample(s->dtype, s->psi, s->n, shots, seed, scratch.p, (uint64_t*)d_out.p, s->stream));
+    CK(cudaMemcpyAsync(out, d_out.p, shots * sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     s->st.launches += 5;
   });
@@ -672,10 +719,10 @@ int qs_apply_dense6(qs_state* s, const double* U) {
     for (int i = 0; i < 4096; ++i) u[i] = cplx(U[2 * i], U[2 * i + 1]);
     std::vector<uint8_t> w(dense6_weight_bytes());
     dense6_prepare_weights(u.data(), w.data());
-    if (!s->d_dense) CK(cudaMalloc(&s->d_dense, w.size()));
+    if (!s->d_dense) CK(dev_malloc(&s->d_dense, w.size()));
     // pageable source: staged before the call returns, copied in stream order
     CK(cudaMemcpyAsync(s->d_dense, w.data(), w.size(), cudaMemcpyHostToDevice, s->stream));
-    CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, kBarrierLimitNs, s->stream));
+    CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, s->wait_limit_ns, s->stream));
     s->st.launches += 1;
     s->st.gate_sweeps += 1;
   });
@@ -730,6 +777,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     s->jit_lr = c->jit_lr;
     s->jit_blocks = c->jit_blocks;
     s->jit_packed = c->jit_packed;
+    s->wait_limit_ns = c->wait_limit_ns ? c->wait_limit_ns : kBarrierLimitNs;
   });
 }
 
@@ -741,6 +789,7 @@ int qs_get_config(qs_state* s, qs_config* c) {
     c->jit_lr = s->jit_lr;
     c->jit_blocks = s->jit_blocks;
     c->jit_packed = s->jit_packed;
+    c->wait_limit_ns = s->wait_limit_ns;
   });
 }
 
@@ -773,12 +822,12 @@ int qs_norm_squared(qs_state* s, double* out) {
 int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im) {
   return guard([&] {
     if (!a || !b || !re || !im) throw InvalidArg{"null argument"};
-    if (a->n != b->n || a->dtype != b->dtype) throw InvalidArg{"states differ in size or dtype"};
+    if (a->n != b->n) throw InvalidArg{"states differ in size"};
     a->materialize();
     b->materialize();
     CK(cudaStreamSynchronize(b->stream));
     CK(cudaMemsetAsync(a->d_acc, 0, 2 * sizeof(double), a->stream));
-    CK(launch_inner(a->dtype, a->psi, b->psi, a->n, a->d_acc, a->stream));
+    CK(launch_inner_mixed(a->dtype, a->psi, b->dtype, b->psi, a->n, a->d_acc, a->stream));
     CK(cudaMemcpyAsync(a->h_acc, a->d_acc, 2 * sizeof(double), cudaMemcpyDeviceToHost, a->stream));
     CK(cudaStreamSynchronize(a->stream));
     a->check_device_error();
@@ -830,8 +879,9 @@ int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nop
     psi->materialize();
     lam->materialize();
     CK(cudaStreamSynchronize(lam->stream));
-    double* d_grad = nullptr;
-    CK(cudaMallocAsync(&d_grad, std::max(1, ngrads) * sizeof(double), psi->stream));
+    AsyncBuf grad_buf(psi->stream);
+    CK(grad_buf.alloc(std::max(1, ngrads) * sizeof(double)));
+    double* d_grad = (double*)grad_buf.p;
     CK(cudaMemsetAsync(d_grad, 0, std::max(1, ngrads) * sizeof(double), psi->stream));
     for (int i = nops - 1; i >= 0; --i) {
       const qs_adj_op& o = ops[i];
@@ -851,7 +901,6 @@ int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nop
       psi->st.gate_sweeps += 2;
     }
     if (ngrads > 0) CK(cudaMemcpyAsync(grads, d_grad, ngrads * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
-    CK(cudaFreeAsync(d_grad, psi->stream));
     CK(cudaStreamSynchronize(psi->stream));
   });
 }

@@ -66,6 +66,11 @@ typedef struct {
   int jit_blocks; /* specialised kernels: 1 double-buffered block per SM, 2 single-buffered
                      blocks per SM, 3 one block of two teams over three buffers */
   int jit_packed; /* specialised kernels: FP32x2 arithmetic on two amplitudes (1) or scalar (0) */
+  unsigned long long wait_limit_ns; /* limit of every bounded device wait of this state's kernels
+                                       (grid barriers of cooperative launches, tensor-core
+                                       completion waits); 0 = the default, 20 s.  A wait that
+                                       expires sets an error word; the call that observes it
+                                       returns QS_ERR_DEVICE and the state stays usable. */
 } qs_config;
 
 typedef struct {
@@ -84,6 +89,11 @@ typedef struct {
 
 /* Library */
 QS_API const char* qs_last_error(void);
+/* Fault injection for tests of the error paths (no counterpart in the reference, whose only
+ * failure handling is catching out-of-memory exceptions in its benchmark driver,
+ * benches/run_benchmarks.py:192-213): the k-th next device or pinned-host allocation made by
+ * the library fails with a CUDA out-of-memory error and allocates nothing (k <= 0: off). */
+QS_API int qs_debug_fail_alloc(int k);
 QS_API int qs_version(void);
 QS_API int qs_device_count(int* out);
 
@@ -151,7 +161,9 @@ QS_API int qs_reset_stats(qs_state* s);
 /* Current layout relabelling: out[p] = physical bit holding layout position p. */
 QS_API int qs_get_pos2bit(qs_state* s, int* out, int n);
 
-/* Reductions in FP64: sum |psi|^2 and <a|b> (states of equal size and dtype). */
+/* Reductions in FP64: sum |psi|^2 and <a|b> (states of equal size; a complex64 and a
+ * complex128 state may be paired, e.g. to measure a single-precision run against a
+ * double-precision one). */
 QS_API int qs_norm_squared(qs_state* s, double* out);
 QS_API int qs_inner_product(qs_state* a, qs_state* b, double* re, double* im);
 
@@ -198,11 +210,15 @@ QS_API int qs_permute_scatter(const void* in, void* out, int dtype, int num_qubi
  * nothing: its program and grid-barrier words live in one fixed 1 MiB device array that
  * every GPU loading the library holds until exit.  Calls whose encoded program exceeds that
  * array (about 20,000 gates) are rejected with an error asking to split them.
+ * psi must be 16-byte aligned device memory of the current device (or managed memory):
+ * the kernel moves amplitudes in 16-byte units; other pointers are rejected with
+ * QS_ERR_INVALID before anything is launched.  Errors name this entry point.
  * The first call on a device looks up the array's device address (with that device
- * current); make it before any stream capture.  All calls share the array: it is reset at
- * the start of each call, and calls that overlap on the GPU (other streams, other host
- * threads) race -- serialise them.  The call returns after the work on `stream` (NULL: the
- * legacy default stream) has finished. */
+ * current) and keeps it for the life of the process; make that first call before any stream
+ * capture, and do not call this entry point again after cudaDeviceReset on that device.
+ * All calls share the array: it is reset at the start of each call, and calls that overlap
+ * on the GPU (other streams, other host threads) race -- serialise them.  The call returns
+ * after the work on `stream` (NULL: the legacy default stream) has finished. */
 QS_API int qs_apply_ops_noalloc(void* psi, int dtype, int num_qubits, const qs_op* ops, int nops, void* stream);
 
 /* LQR flat tiling of a depth-sorted gate list (host only; replaces the Python loops of
@@ -258,6 +274,8 @@ typedef struct {
   int chunk;         /* groups per work item (>= 1) */
   int threads;       /* threads per block: 256 or 512 */
   int blocks_per_sm; /* cap on resident blocks per SM (0: as many as fit) */
+  int pad;
+  unsigned long long wait_limit_ns; /* limit of the kernel's dependency waits (0: 10 s) */
 } qs_batch_config;
 /* Plan and encode the batch, allocate its device program, arena and outputs (cfg NULL:
  * m 13, small_max 13, chunk 4, 256 threads). */

@@ -73,3 +73,42 @@ def ops_of(qc):
         U = op.to_matrix()
         out.append(("1q", qs[0], U) if len(qs) == 1 else ("2q", qs[0], qs[1], U))
     return out
+
+
+# angles at which a rotation's cosine or sine (nearly) vanishes, and phases near 0 and 2 pi
+ADVERSARIAL_ANGLES = (np.pi - 1e-7, np.pi + 1e-7, 1e-7, 2 * np.pi - 1e-7, np.pi - 1e-5, np.pi + 1e-4,
+                      np.pi - 1e-3, 3 * np.pi - 1e-5)
+ADVERSARIAL_PHASES = (1e-7, 2 * np.pi - 1e-7, np.pi + 1e-7, -1e-7, 1e-5)
+
+
+def adversarial_angles(n, depth, seed):
+    """Layers of RX / RY / RZ at angles where cos(t/2) or sin(t/2) is tiny, H on a few qubits,
+    a CX ladder (no two rotations on one qubit fuse), and CP at phases near 0 and 2 pi: long
+    runs of such gates land in one pass of the executor."""
+    import random
+    rng = random.Random(seed)
+    from frontierlabproject_b200.circuit import QuantumCircuit
+    qc = QuantumCircuit(n)
+    for q in range(n):
+        qc.h(q)
+    for layer in range(depth):
+        for q in range(n):
+            t = rng.choice(ADVERSARIAL_ANGLES)
+            g = rng.randrange(4)
+            if g == 0:
+                qc.rx(t, q)
+            elif g == 1:
+                qc.ry(t, q)
+            elif g == 2:
+                qc.rz(t, q)
+            else:
+                qc.rx(t, q)
+                qc.ry(rng.choice(ADVERSARIAL_ANGLES), q)
+        start = layer % 2
+        for q in range(start, n - 1, 2):
+            qc.cx(q, q + 1)
+        for _ in range(max(1, n // 4)):
+            a, b = rng.sample(range(n), 2)
+            qc.cp(rng.choice(ADVERSARIAL_PHASES), a, b)
+        qc.rx(np.pi - 1e-5, layer % n)
+    return qc

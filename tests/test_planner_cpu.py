@@ -110,3 +110,15 @@ def test_abi_validation_messages(native_lib):
         _OpBatch([("1q", 1)], 0)
     with pytest.raises(RuntimeError, match="U must be a 2x2 matrix"):
         _OpBatch([("1q", 1, np.eye(3))], 0)
+
+
+@pytest.mark.parametrize("n,seed", [(13, 0), (16, 1)])
+def test_plan_emulation_adversarial_angles(native_lib, n, seed):
+    # rotations whose cosine or sine nearly vanishes: the per-pass scalar extraction keeps the
+    # complex64 state inside the single-precision range (no overflow, no underflow)
+    from tests.cases import adversarial_angles
+    qc = adversarial_angles(n, 12, seed)
+    psi, _, _ = _emulate(qc, 0)
+    assert np.all(np.isfinite(psi))
+    assert O.infidelity(O.simulate(qc), psi) <= 1e-5
+    assert abs(np.vdot(psi.astype(np.complex128), psi).real - 1.0) <= 1e-4

@@ -17,6 +17,7 @@ import pytest
 from frontierlabproject_b200 import _native as N
 from frontierlabproject_b200 import circuits as C
 from frontierlabproject_b200.qgpusim_cuda import Statevector, StatevectorF32, _OpBatch
+from oracle import statevector as O
 from tests.cases import ops_of
 
 pytestmark = pytest.mark.gpu
@@ -47,6 +48,7 @@ def test_noalloc_matches_allocating_entry_point(dt):
     dev = torch.from_numpy(psi0.copy()).cuda()
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream().cuda_stream
+    oracle = psi0.astype(np.complex128)
     for call, seed in enumerate((1, 2)):  # two calls in a row
         ops = _ops(seed, n)
         sv.apply_tile_cooperative(ops)
@@ -57,6 +59,13 @@ def test_noalloc_matches_allocating_entry_point(dt):
         assert rc == 0, N.lib().qs_last_error().decode()
         got = dev.cpu().numpy()
         assert np.max(np.abs(got.astype(np.complex128) - ref)) <= TOL[dt], f"call {call + 1}"
+        # and against the FP64 oracle (the reference's per-gate arithmetic)
+        for op in ops:
+            if op[0] == "1q":
+                O.apply_1q(oracle, op[2], op[1])
+            else:
+                O.apply_2q(oracle, op[3], op[1], op[2])
+        assert np.max(np.abs(got.astype(np.complex128) - oracle)) <= TOL[dt], f"call {call + 1} vs oracle"
 
 
 def test_noalloc_rejects_programs_beyond_the_workspace():
@@ -68,3 +77,24 @@ def test_noalloc_rejects_programs_beyond_the_workspace():
     rc = N.lib().qs_apply_ops_noalloc(ctypes.c_void_p(dev.data_ptr()), 0, n, batch.ptr, len(batch), None)
     assert rc != 0
     assert b"static workspace" in N.lib().qs_last_error()
+
+
+def test_noalloc_rejects_unaligned_and_host_pointers():
+    # checked on the host before anything is launched: the kernel moves 16-byte units
+    import torch
+    n = 14
+    dev = torch.zeros((1 << n) + 1, dtype=torch.complex64, device="cuda")
+    batch = _OpBatch(_ops(4, n), 0)
+    rc = N.lib().qs_apply_ops_noalloc(ctypes.c_void_p(dev[1:].data_ptr()), 0, n, batch.ptr, len(batch), None)
+    assert rc == N.QS_ERR_INVALID
+    assert b"16-byte aligned" in N.lib().qs_last_error()
+    host = np.zeros(1 << n, dtype=np.complex64)
+    rc = N.lib().qs_apply_ops_noalloc(ctypes.c_void_p(host.ctypes.data), 0, n, batch.ptr, len(batch), None)
+    assert rc == N.QS_ERR_INVALID
+    assert b"qs_apply_ops_noalloc" in N.lib().qs_last_error()
+    # op validation errors name this entry point
+    bad = np.zeros(1, dtype=N.OP_DTYPE)
+    bad["kind"] = 7
+    rc = N.lib().qs_apply_ops_noalloc(ctypes.c_void_p(dev.data_ptr()), 0, n, bad.ctypes.data, 1, None)
+    assert rc == N.QS_ERR_INVALID
+    assert N.lib().qs_last_error().startswith(b"qs_apply_ops_noalloc: unknown op kind")
