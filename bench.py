@@ -12,10 +12,15 @@ tile, per reorder and for the final read-out, as the reference schedule executes
 ``circuit_time_s`` is t itself.  ``value`` is device-timed (CUDA events on the executor's
 stream, inputs resident); ``e2e`` is the same metric through ``run_custom_backend`` with a
 pinned host result (8 GiB device->host per step) and the host-side op preparation.
+``fidelity_err_vs_fp64`` = 1 - |<psi64|psi32>|^2 of the timed circuit against the complex128
+executor on the same GPU; ``n33`` times the same circuit family at n=33 (64 GiB state);
+``first_call_s`` is the cold start of the first step (planning, kernel compiles, graph capture).
 
-``--impl reference`` times the CPU implementation of the reference algorithm (one
-full-state pass per gate, out-of-place scatter per reorder; the C/OpenMP restatement in
-oracle/) on a bounded sample of the same workload and extrapolates to the whole schedule.
+``--impl reference`` times the CPU implementation of the reference algorithm (one full-state
+pass per gate, out-of-place scatter per reorder: the C/OpenMP restatement of the reference's
+kernels in oracle/) on the host cores; each step runs a sample of the schedule's work units
+(fused gates and reorders, spread over the whole schedule) on the full state, and the value is
+the sampled units' share of B_alg divided by their measured time.
 """
 from __future__ import annotations
 
@@ -117,88 +122,112 @@ def prepared_tiles(qc, plan, np_dtype):
     return out
 
 
-def traffic_from_profile():
-    """DRAM bytes per pass-kernel launch recorded from an ncu capture (profiles/)."""
-    p = os.path.join(HERE, "profiles", "pass_kernel_random_n30.md")
-    try:
-        for line in open(p):
-            if line.startswith("traffic_bytes_per_sweep:"):
-                return float(line.split(":")[1])
-    except Exception:
-        pass
-    return None
+class CpuReference:
+    """The reference algorithm on the host cores (oracle/cpu_kernels.c, C/OpenMP): one full-state
+    pass per fused gate, an out-of-place scatter per reorder.  Loads no library of the package.
+    Work units are the schedule's fused gates and reorders in execution order."""
 
+    def __init__(self, qc, plan, n_cpu: int):
+        import ctypes
+        from oracle import build as ob
+        from oracle import statevector as O
+        self.ct = ctypes
+        lib = ctypes.CDLL(ob.build())
+        lib.qo_apply_1q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        lib.qo_apply_2q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        lib.qo_permute_scatter_c64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        lib.qo_max_threads.restype = ctypes.c_int
+        self.lib = lib
+        self.threads = lib.qo_max_threads()
+        self.n = qc.num_qubits
+        self.n_cpu = n_cpu
+        qindex = {q: qc.find_bit(q).index for q in qc.qubits}
+        units = []
+        layout = list(range(self.n))
+        for t in plan:
+            if list(t.layout) != layout:
+                units.append(("perm", layout, list(t.layout)))
+                layout = list(t.layout)
+            for op in O.fuse_ops(O.tile_ops_from_tile(t, qindex, np.complex64)):
+                units.append(op)
+        self.units = units
+        self.gates = sum(1 for u in units if u[0] != "perm")
+        self.reorders = len(units) - self.gates
+        self.psi = np.zeros(1 << n_cpu, dtype=np.complex64)
+        self.psi[0] = 1
+        self.tmp = np.empty_like(self.psi)
 
-def cpu_reference_sample(qc, plan, n_cpu: int, budget_s: float):
-    """Time the C/OpenMP restatement of the reference kernels on a bounded sample of the
-    schedule (leading fused ops and reorders) and extrapolate to the whole schedule."""
-    import ctypes
-    from oracle import build as ob
-    from frontierlabproject_b200.backend import fuse_tile_ops, tile_ops_for
-    lib = ctypes.CDLL(ob.build())
-    lib.qo_apply_1q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
-    lib.qo_apply_2q_c64.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
-    lib.qo_permute_scatter_c64.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
-    lib.qo_max_threads.restype = ctypes.c_int
-    threads = lib.qo_max_threads()
-    qmap = {q: qc.find_bit(q).index for q in qc.qubits}
-    n = qc.num_qubits
-    fused = []
-    for t in plan:
-        fused.extend(fuse_tile_ops(tile_ops_for(t, qmap, np.complex64)))
-    G = len(fused)
-    psi = np.zeros(1 << n_cpu, dtype=np.complex64)
-    psi[0] = 1
-    tmp = np.empty_like(psi)
-    t_gate = []
-    t0 = time.perf_counter()
-    k = 0
-    while time.perf_counter() - t0 < budget_s * 0.8 and k < len(fused):
-        op = fused[k]
-        U = np.ascontiguousarray(op[-1], np.complex64)
-        q0 = min(op[1], n_cpu - 1)
-        s = time.perf_counter()
-        if op[0] == "1q":
-            lib.qo_apply_1q_c64(psi.ctypes.data, n_cpu, q0, U.ctypes.data)
+    def run_unit(self, u) -> None:
+        n = self.n_cpu
+        fold = lambda q: q if q < n else n - 1 - (q - n) % n  # only when the sample state is smaller
+        if u[0] == "perm":
+            new_pos = {q: p for p, q in enumerate(u[2])}
+            mp = [new_pos[u[1][p]] for p in range(self.n)]
+            if n < self.n:
+                mp = list(np.random.default_rng(len(self.units)).permutation(n))
+            mp = np.asarray(mp[:n], dtype=np.int32)
+            self.lib.qo_permute_scatter_c64(self.psi.ctypes.data, self.tmp.ctypes.data, n, mp.ctypes.data)
+            self.psi, self.tmp = self.tmp, self.psi
+        elif u[0] == "1q":
+            U = np.ascontiguousarray(u[2], np.complex64)
+            self.lib.qo_apply_1q_c64(self.psi.ctypes.data, n, fold(u[1]), U.ctypes.data)
         else:
-            q1 = min(op[2], n_cpu - 1)
+            U = np.ascontiguousarray(u[3], np.complex64)
+            q0, q1 = fold(u[1]), fold(u[2])
             if q1 == q0:
-                q1 = (q0 + 1) % n_cpu
-            lib.qo_apply_2q_c64(psi.ctypes.data, n_cpu, q0, q1, U.ctypes.data)
-        t_gate.append(time.perf_counter() - s)
-        k += 1
-    mp = np.random.default_rng(0).permutation(n_cpu).astype(np.int32)
-    s = time.perf_counter()
-    lib.qo_permute_scatter_c64(psi.ctypes.data, tmp.ctypes.data, n_cpu, mp.ctypes.data)
-    t_perm = time.perf_counter() - s
-    scale = float(1 << (n - n_cpu))
-    layouts = [list(range(n))] + [list(t.layout) for t in plan]
+                q1 = (q0 + 1) % n
+            self.lib.qo_apply_2q_c64(self.psi.ctypes.data, n, q0, q1, U.ctypes.data)
+
+    def sample(self, k: int, step: int):
+        """k work units spread over the whole schedule (offset by step): (seconds, units run)."""
+        U = len(self.units)
+        off = (step * 0.6180339887498949) % 1.0
+        idx = sorted({min(U - 1, int((j + off) * U / k)) for j in range(k)})
+        t0 = time.perf_counter()
+        for i in idx:
+            self.run_unit(self.units[i])
+        return time.perf_counter() - t0, len(idx)
+
+    def describe(self, units_run: int, steps: int) -> str:
+        st = (f"{units_run} work units ({steps} samples spread over the schedule's {self.gates} fused gates "
+              f"+ {self.reorders} reorders) on the full {self.n_cpu}-qubit complex64 state")
+        if self.n_cpu != self.n:
+            st += f" (host memory limited the sample state to {self.n_cpu} of {self.n} qubits)"
+        return st
+
+
+def cpu_rate(ref: "CpuReference", b_alg_n: float, t: float, units: int) -> float:
+    """GB/s of algorithmic bytes: the sampled units' share of B_alg over their time."""
+    return (units / len(ref.units)) * b_alg_n / t / 1e9
+
+
+def run_reference_arm(args, rank, world):
+    from frontierlabproject_b200 import circuits as C
+    from frontierlabproject_b200.transpiler import tile_circuit
+    qc = C.random_layered(args.n, args.depth, args.seed)
+    _, plan = tile_circuit(qc, args.nl, native=False)  # the Python restatement of the LQR pass
+    layouts = [list(range(args.n))] + [list(t.layout) for t in plan]
     R = sum(1 for a, b in zip(layouts[:-1], layouts[1:]) if a != b)
-    t_total = (np.mean(t_gate) * G + t_perm * R) * scale
-    sample = (f"{len(t_gate)} leading fused gate passes + 1 reorder of the schedule at n={n_cpu}, "
-              f"extrapolated to {G} gate passes + {R} reorders" + (f" and scaled by 2^{n - n_cpu}" if n_cpu != n else ""))
-    return t_total, threads, sample
-
-
-def run_reference_arm(args, rank):
-    qc, plan, R = build_workload(args.n, args.depth, args.nl, args.seed)
     n_cpu = choose_cpu_n(args.n)
-    sweep = 2 * (1 << args.n) * 8
-    b_alg = (len(plan) + R + 1) * sweep
-    times = []
-    threads, sample = None, None
-    for i in range(args.warmup + args.steps):
-        t, threads, sample = cpu_reference_sample(qc, plan, n_cpu, budget_s=args.cpu_budget)
-        if i >= args.warmup:
-            times.append(t)
-    t = float(np.mean(times))
-    v = b_alg / t / 1e9
-    line = {"metric": METRIC, "value": v, "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "circuit_time_s": t,
-            "config": config_of(args, plan, R),
-            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+    ref = CpuReference(qc, plan, n_cpu)
+    b_alg = (len(plan) + R + 1) * 2 * (1 << n_cpu) * 8
+    for i in range(args.warmup):
+        ref.sample(args.ref_units, i)
+    times, units = [], 0
+    for i in range(args.steps):
+        t, k = ref.sample(args.ref_units, args.warmup + i)
+        times.append(t)
+        units += k
+    t_tot = float(np.sum(times))
+    v = cpu_rate(ref, b_alg, t_tot, units)
+    t_circuit = t_tot / units * len(ref.units) * (1 << (args.n - n_cpu))
+    sample = ref.describe(units, args.steps)
+    line = {"metric": METRIC, "value": v, "unit": "GB/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_tot / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": config_of(args, plan, R, world),
+            "circuit_time_s_extrapolated": t_circuit,
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": ref.threads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -357,6 +386,54 @@ def dense_bench(n: int = 30, reps: int = 10, seed: int = 0) -> dict:
             "infidelity_vs_fp64_n18": 1.0 - fid, "precision": "BF16 high+low split, 3 products, FP32 accumulation"}
 
 
+def n33_bench(args, hbm_peak) -> dict:
+    """The same circuit family at n=33 (64 GiB complex64 state), depth 100, the reference
+    schedule at nL=20: device time per circuit (CUDA events), B_alg / t and the sweep count."""
+    import torch
+    from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
+    n = 33
+    qc, plan, R = build_workload(n, args.depth, args.nl, args.seed)
+    tiles = prepared_tiles(qc, plan, np.complex64)
+    sv = StatevectorF32(n)
+    sv.set_config(m=args.m, k=args.k, jit=args.jit, jit_lr=args.jit_lr, jit_blocks=args.jit_blocks,
+                  jit_packed=args.jit_packed)
+    stream = torch.cuda.ExternalStream(sv.stream)
+
+    def run():
+        sv.reset()
+        layout = list(range(n))
+        for lay, batch in tiles:
+            if lay != layout:
+                sv.permute(layout, lay)
+                layout = lay
+            if batch is not None:
+                sv.apply_tile_graphed(batch)
+        sv.materialize()
+
+    t0 = time.perf_counter()
+    run()
+    sv.synchronize()
+    first = time.perf_counter() - t0
+    sv.reset_stats()
+    reps = 2
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(reps):
+        run()
+    ev[1].record(stream)
+    sv.synchronize()
+    t = ev[0].elapsed_time(ev[1]) / reps / 1e3
+    st = sv.stats()
+    sweep = 2 * (1 << n) * 8
+    b_alg = (len(plan) + R + 1) * sweep
+    sv.close()
+    return {"workload": f"random circuit n={n} depth={args.depth} complex64, reference LQR schedule nL={args.nl} "
+                        f"({len(plan)} tiles, {R} reorders), seed {args.seed}",
+            "circuit_time_s": t, "value_gbs": b_alg / t / 1e9, "hbm_frac_alg": b_alg / t / 1e9 / hbm_peak,
+            "sweeps_per_circuit": (st["sweeps"] + st["gate_sweeps"]) / reps,
+            "reference_sweeps_per_circuit": len(plan) + R + 1, "first_call_s": first, "reps": reps}
+
+
 def choose_cpu_n(n: int) -> int:
     try:
         import psutil
@@ -369,13 +446,14 @@ def choose_cpu_n(n: int) -> int:
     return m
 
 
-def config_of(args, plan, R):
+def config_of(args, plan, R, world=1):
     return {"workload": f"random circuit n={args.n} depth={args.depth} complex64 from |0>, reference LQR "
                         f"schedule nL={args.nl} ({len(plan)} tiles, {R} reorders), seed {args.seed}",
             "n": args.n, "depth": args.depth, "nL": args.nl, "tile_mode": args.mode,
             "l2": (f"state ({(8 << args.n) / 2**30:g} GiB) > L2 (126 MB): every sweep streams from HBM, "
                    "no flush needed" if (8 << args.n) > 126e6 else
-                   f"state ({(8 << args.n) / 2**20:g} MiB) fits in L2: not an HBM measurement")}
+                   f"state ({(8 << args.n) / 2**20:g} MiB) fits in L2: not an HBM measurement"),
+            "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def main():
@@ -402,6 +480,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--batch-count", type=int, default=512, help="instances of the batched variational workload")
+    ap.add_argument("--no-fidelity", action="store_true")
+    ap.add_argument("--n33", type=int, default=1, help="also time the n=33 circuit (64 GiB state)")
+    ap.add_argument("--ref-units", type=int, default=16, help="reference arm: work units per step")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -409,7 +490,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         if rank == 0:
-            run_reference_arm(args, rank)
+            run_reference_arm(args, rank, world)
         return
 
     import torch
@@ -454,7 +535,14 @@ def main():
         ev[1].record(stream)
 
     mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    for _ in range(args.warmup):
+    # cold start: the first step plans the schedule, compiles its kernels and captures the graph
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    step(mk())
+    sv.synchronize()
+    first_call_s = time.perf_counter() - t0
+    first = sv.stats()
+    for _ in range(max(0, args.warmup - 1)):
         step(mk())
     sv.synchronize()
     sv.reset_stats()
@@ -481,9 +569,35 @@ def main():
     value = whole_job_rate(b_alg, ms_step / 1e3, world) / 1e9
     sweeps_step = (st["sweeps"] + st["gate_sweeps"]) / args.steps
     achieved = sweeps_step * sweep / (pass_ms / args.steps / 1e3) / 1e9
-    traffic = traffic_from_profile()
     launches_step = 1 + (st["sweeps"] - st["perm_sweeps"]) / args.steps + (1 if st["perm_sweeps"] else 0) \
         if args.mode == "graphed" else 1 + st["launches"] / args.steps
+
+    # ---- fidelity of the timed circuit against double precision on the same GPU ----
+    fid = None
+    if not args.no_fidelity:
+        from frontierlabproject_b200.qgpusim_cuda import Statevector
+        step(mk())
+        sv.synchronize()
+        sv64 = Statevector(n)
+        t0 = time.perf_counter()
+        layout = list(range(n))
+        for lay, batch in prepared_tiles(qc, plan, np.complex128):
+            if lay != layout:
+                sv64.permute(layout, lay)
+                layout = lay
+            if batch is not None:
+                sv64.apply_tile_graphed(batch)
+        sv64.synchronize()
+        t64 = time.perf_counter() - t0
+        ov = sv64.inner(sv)
+        n32, n64 = sv.norm_squared(), sv64.norm_squared()
+        fid = {"fidelity_err_vs_fp64": max(0.0, 1.0 - abs(ov) ** 2 / (n32 * n64)),
+               "norm_c64": n32, "norm_c128": n64,
+               "reference": "the same schedule through the complex128 executor (generic pass kernel) on the same "
+                            "GPU; 1 - |<psi64|psi32>|^2 / (|psi32|^2 |psi64|^2), FP64 on the device",
+               "c128_run_s": t64}
+        sv64.close()
+        del sv64
 
     # ---- end to end through the public API (pinned host result) ----
     e2e = None
@@ -502,6 +616,9 @@ def main():
         h2d = sum(b.arr.nbytes + sum(k.nbytes for k in b._keep) for _, b in tiles if b is not None)
         e2e = {"value": whole_job_rate(b_alg, te, world) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int((1 << n) * 8), "circuit_time_s": te}
+        del out
+    sv.close()
+    del sv
 
     adj = None
     if not args.no_adjoint:
@@ -512,29 +629,49 @@ def main():
     den = None
     if not args.no_dense:
         den = dense_bench(n)
+    big = None
+    if args.n33 and world == 1:
+        big = n33_bench(args, hbm_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        t_cpu, threads, sample = cpu_reference_sample(qc, plan, choose_cpu_n(n), args.cpu_budget)
-        cpu = {"value": b_alg / t_cpu / 1e9, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample,
-               "circuit_time_s": t_cpu}
+        ref = CpuReference(qc, plan, choose_cpu_n(n))
+        b_alg_cpu = (len(plan) + R + 1) * 2 * (1 << ref.n_cpu) * 8
+        ref.sample(4, 0)  # warm-up: first touch of the host state
+        t_cpu, units, k = 0.0, 0, 0
+        while t_cpu < args.cpu_budget:
+            t, u = ref.sample(8, 1 + k)
+            t_cpu += t
+            units += u
+            k += 1
+        v = cpu_rate(ref, b_alg_cpu, t_cpu, units)
+        cpu = {"value": v, "unit": "GB/s", "cores": ref.threads, "kind": "port", "sample": ref.describe(units, k),
+               "seconds": t_cpu,
+               "circuit_time_s_extrapolated": t_cpu / units * len(ref.units) * (1 << (n - ref.n_cpu))}
+        del ref
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c64", "data": "synthetic",
                 "circuit_time_s": ms_step / 1e3,
-                "config": dict(config_of(args, plan, R), parallelism="replicas" if world > 1 else "single GPU"),
+                "config": config_of(args, plan, R, world),
                 "sweeps_per_step": sweeps_step, "reference_sweeps_per_step": len(plan) + R + 1,
+                "fidelity_err_vs_fp64": fid["fidelity_err_vs_fp64"] if fid else None, "fidelity": fid,
+                "first_call_s": first_call_s, "first_call_compile_s": first["jit_compile_ms"] / 1e3,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                             "frac": achieved / hbm_peak, "traffic": traffic,
+                             "frac": achieved / hbm_peak, "traffic": None,
+                             "traffic_note": "DRAM bytes per launch come from ncu captures of this kernel "
+                                             "(profiles/), not from this run",
                              "kernel": ("qp_<key>_<pass> (pass kernel specialised at plan time)"
-                                        if st["jit_compile_ms"] or (args.mode == "graphed" and args.jit >= 0 and n >= 20)
+                                        if first["jit_compile_ms"] or (args.mode == "graphed" and args.jit >= 0
+                                                                       and n >= 20)
                                         else "pass_kernel<float,5>"),
                              "peak_kind": peak_kind,
                              "algorithmic_bytes_per_sweep": sweep},
                 "gpu_launches": int(round(launches_step * args.steps)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "adjoint": adj, "batch": bat, "dense_tc": den}
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "n33": big, "adjoint": adj, "batch": bat,
+                "dense_tc": den}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

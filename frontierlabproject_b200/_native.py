@@ -37,7 +37,8 @@ class QsConfig(ctypes.Structure):
 class QsStats(ctypes.Structure):
     _fields_ = [(name, c_ulonglong) for name in
                 ("gates", "sweeps", "perm_sweeps", "gate_sweeps", "launches", "graph_replays",
-                 "graph_builds", "flushes", "permutes", "plans", "jit_compile_ms")]
+                 "graph_builds", "flushes", "permutes", "plans", "jit_compile_ms", "jit_modules",
+                 "jit_disk_hits")]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}

@@ -1,11 +1,17 @@
 // Plan-time specialisation of pass kernels (see jit.h).
 #include "jit.h"
 
+#include <cerrno>
 #include <cuda.h>
 #include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
 #include <functional>
 #include <cstring>
 #include <list>
@@ -29,6 +35,7 @@ struct Nvrtc {
   int (*log_size)(void*, size_t*) = nullptr;
   int (*log)(void*, char*) = nullptr;
   int (*destroy)(void**) = nullptr;
+  int (*version)(int*, int*) = nullptr;
   std::string why;
   bool ok = false;
   Nvrtc() {
@@ -45,6 +52,7 @@ struct Nvrtc {
     log_size = (decltype(log_size))dlsym(h, "nvrtcGetProgramLogSize");
     log = (decltype(log))dlsym(h, "nvrtcGetProgramLog");
     destroy = (decltype(destroy))dlsym(h, "nvrtcDestroyProgram");
+    version = (decltype(version))dlsym(h, "nvrtcVersion");
     ok = create && compile && cubin_size && cubin && log_size && log && destroy;
     if (!ok) why = "NVRTC symbols missing";
   }
@@ -871,6 +879,13 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
 
 namespace {
 
+// NVRTC options; entry 3 is replaced by the include path of the device headers.  No line
+// tables: they add a quarter to the compile time and nothing to the code.
+constexpr int kNumOpts = 7;
+const char* const kCompileOpts[kNumOpts] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device",
+                                            "-I<csrc>", "--extra-device-vectorization", "--disable-warnings",
+                                            "--ptxas-options=-v"};
+
 bool compile_source(const std::string& src, std::vector<char>* cubin, std::string* log, bool verbose = false) {
   Nvrtc& nv = nvrtc();
   void* prog = nullptr;
@@ -879,10 +894,10 @@ bool compile_source(const std::string& src, std::vector<char>* cubin, std::strin
     return false;
   }
   const std::string inc = "-I" + csrc_dir();
-  // no line tables: they add a quarter to the compile time and nothing to the code
-  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", inc.c_str(),
-                        "--extra-device-vectorization", "--disable-warnings", "--ptxas-options=-v"};
-  const int rc = nv.compile(prog, verbose ? 7 : 6, opts);
+  const char* opts[kNumOpts];
+  for (int i = 0; i < kNumOpts; ++i) opts[i] = kCompileOpts[i];
+  opts[3] = inc.c_str();
+  const int rc = nv.compile(prog, verbose ? kNumOpts : kNumOpts - 1, opts);
   size_t ls = 0;
   nv.log_size(prog, &ls);
   std::string lg(ls, '\0');
@@ -901,6 +916,99 @@ bool compile_source(const std::string& src, std::vector<char>* cubin, std::strin
 
 std::mutex g_mu;
 std::list<std::shared_ptr<JitKernels>> g_cache;  // most recent first
+
+// ---- compiled kernels kept on disk across processes -----------------------------------
+// A cubin is stored under the FNV-1a hash of everything that determines it: the generated
+// source, the device headers it includes, the compile options and the NVRTC version.
+// $QSIM_JIT_CACHE names the directory ("0" or "off": no disk cache); by default
+// $XDG_CACHE_HOME/qsim_b200/jit or ~/.cache/qsim_b200/jit.
+uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ull) {
+  for (unsigned char c : s) {
+    h ^= c;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+std::string read_file(const std::string& path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return std::string();
+  std::ostringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+std::string disk_cache_dir() {
+  const char* e = std::getenv("QSIM_JIT_CACHE");
+  if (e) {
+    if (!*e || !std::strcmp(e, "0") || !std::strcmp(e, "off")) return std::string();
+    return e;
+  }
+  const char* x = std::getenv("XDG_CACHE_HOME");
+  const char* home = std::getenv("HOME");
+  std::string base = (x && *x) ? std::string(x) : (home && *home ? std::string(home) + "/.cache" : std::string());
+  return base.empty() ? base : base + "/qsim_b200/jit";
+}
+
+bool make_dirs(const std::string& dir) {
+  std::string cur;
+  size_t i = 0;
+  while (i <= dir.size()) {
+    const size_t j = dir.find('/', i);
+    cur = dir.substr(0, j == std::string::npos ? dir.size() : j);
+    if (!cur.empty()) {
+      struct stat st;
+      if (stat(cur.c_str(), &st) != 0 && mkdir(cur.c_str(), 0755) != 0 && errno != EEXIST) return false;
+    }
+    if (j == std::string::npos) break;
+    i = j + 1;
+  }
+  return true;
+}
+
+// the part of a kernel's cache key that does not depend on its source
+uint64_t disk_key_base(const char* const* opts, int nopts) {
+  static uint64_t base = 0;
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    std::string k = read_file(csrc_dir() + "/qsim.h") + read_file(csrc_dir() + "/pass_body.cuh");
+    for (int i = 0; i < nopts; ++i) k += std::string("\n") + opts[i];
+    int major = 0, minor = 0;
+    if (nvrtc().version) nvrtc().version(&major, &minor);
+    k += "\nnvrtc " + std::to_string(major) + "." + std::to_string(minor);
+    base = fnv1a(k);
+  });
+  return base;
+}
+
+std::string disk_path(const std::string& dir, const std::string& src, uint64_t base) {
+  char name[40];
+  std::snprintf(name, sizeof(name), "/qp_%016llx.cubin", (unsigned long long)fnv1a(src, base));
+  return dir + name;
+}
+
+bool disk_load(const std::string& path, std::vector<char>* cubin) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) return false;
+  const std::streamsize n = f.tellg();
+  if (n <= 0) return false;
+  cubin->resize((size_t)n);
+  f.seekg(0);
+  return (bool)f.read(cubin->data(), n);
+}
+
+void disk_store(const std::string& path, const std::vector<char>& cubin) {
+  const size_t slash = path.rfind('/');
+  if (slash == std::string::npos || !make_dirs(path.substr(0, slash))) return;
+  const std::string tmp = path + "." + std::to_string((long long)getpid()) + ".tmp";
+  {
+    std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+    if (!f) return;
+    f.write(cubin.data(), (std::streamsize)cubin.size());
+    if (!f) { std::remove(tmp.c_str()); return; }
+  }
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
 
 }  // namespace
 
@@ -946,13 +1054,23 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg_in
   std::vector<int> ok(nchunk, 0);
   std::vector<std::pair<int, int>> range(nchunk);
   for (int c = 0; c < nchunk; ++c) range[c] = {npass * c / nchunk, npass * (c + 1) / nchunk};
+  const std::string dir = disk_cache_dir();
+  const uint64_t base = dir.empty() ? 0 : disk_key_base(kCompileOpts, kNumOpts - 1);
+  std::vector<int> hit(nchunk, 0);
   {
     std::vector<std::thread> th;
     for (int c = 0; c < nchunk; ++c)
       th.emplace_back([&, c] {
         try {
-          ok[c] = compile_source(jit_source(prog, range[c].first, range[c].second, key, cfg, &splats[c]), &cubins[c],
-                                 &logs[c]);
+          const std::string src = jit_source(prog, range[c].first, range[c].second, key, cfg, &splats[c]);
+          const std::string path = dir.empty() ? std::string() : disk_path(dir, src, base);
+          if (!path.empty() && disk_load(path, &cubins[c])) {
+            ok[c] = 1;
+            hit[c] = 1;
+            return;
+          }
+          ok[c] = compile_source(src, &cubins[c], &logs[c]);
+          if (ok[c] && !path.empty()) disk_store(path, cubins[c]);
         } catch (const std::exception& e) {
           logs[c] = e.what();
         }
@@ -964,6 +1082,8 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg_in
   auto k = std::make_shared<JitKernels>();
   k->key = key;
   k->blocks = cfg.blocks;
+  for (int c = 0; c < nchunk; ++c) k->disk_hits += hit[c];
+  k->chunks = nchunk;
   k->cbase.resize(npass);
   k->ccount.resize(npass);
   for (int p = 0; p < npass; ++p) pass_coef_range(prog.bytes.data(), p, &k->cbase[p], &k->ccount[p]);

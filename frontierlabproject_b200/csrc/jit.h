@@ -36,6 +36,8 @@ struct JitKernels {
   uint64_t key = 0;
   int blocks = 1;
   double compile_seconds = 0.0;
+  int chunks = 0;       // compiled modules
+  int disk_hits = 0;    // of which read from the on-disk cache
   ~JitKernels();
 };
 
@@ -50,7 +52,9 @@ uint64_t jit_key(const Program& prog, const JitConfig& cfg);
 std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64_t key, const JitConfig& cfg,
                        std::vector<std::vector<uint32_t>>* splats = nullptr);
 
-// Compile (cached) the kernels of every pass of a complex64 program.
+// Compile (cached) the kernels of every pass of a complex64 program.  Compiled modules are
+// also kept on disk across processes ($QSIM_JIT_CACHE, default ~/.cache/qsim_b200/jit; "off"
+// disables it), keyed by their source, the device headers, the options and NVRTC's version.
 std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
 
 // Launch the specialised kernel of pass p (one launch per pass, no grid barrier).

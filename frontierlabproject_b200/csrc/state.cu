@@ -242,7 +242,11 @@ struct qs_state {
         jc.packed = jit_packed != 0;
         jk = jit_get(prog, jc);
         st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
+        st.jit_modules += (unsigned long long)jk->chunks;
+        st.jit_disk_hits += (unsigned long long)jk->disk_hits;
         jk->compile_seconds = 0.0;  // counted once
+        jk->chunks = 0;
+        jk->disk_hits = 0;
       }
       const uint64_t skey = jk ? jk->key : prog.structure_hash;
       const uint64_t key = skey ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^

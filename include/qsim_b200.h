@@ -85,6 +85,8 @@ typedef struct {
   unsigned long long permutes;       /* permute() calls */
   unsigned long long plans;          /* pass plans computed (cache misses) */
   unsigned long long jit_compile_ms; /* host time spent compiling specialised kernels */
+  unsigned long long jit_modules;    /* kernel modules prepared for specialised programs */
+  unsigned long long jit_disk_hits;  /* of which read from the on-disk kernel cache */
 } qs_stats;
 
 /* Library */

@@ -282,3 +282,50 @@ def adjoint_gradient(qc, a, b):
         else:
             apply_2q(psi, Ud, qs[0], qs[1]); apply_2q(lam, Ud, qs[0], qs[1])
     return E, np.array(grads[::-1])
+
+
+# ------------------------------------------------------------------------------------
+# the same gate-by-gate simulation through the C/OpenMP restatement (oracle/cpu_kernels.c)
+# ------------------------------------------------------------------------------------
+def simulate_c(qc, dtype=np.complex128, psi0=None) -> np.ndarray:
+    """``simulate`` run by the C/OpenMP kernels (one pass per gate, all host cores): the FP64
+    checker for states too large for the numpy loop."""
+    import ctypes
+    from . import build as _build
+    lib = ctypes.CDLL(_build.build())
+    suf = "c128" if np.dtype(dtype) == np.complex128 else "c64"
+    real = np.float64 if suf == "c128" else np.float32
+    run = getattr(lib, f"qo_run_ops_{suf}")
+    run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                    ctypes.c_void_p, ctypes.c_void_p]
+    n = qc.num_qubits
+    qindex = {q: qc.find_bit(q).index for q in qc.qubits}
+    kinds, q0s, q1s, mats = [], [], [], []
+    for ins in qc.data:
+        op = ins.operation
+        if not hasattr(op, "to_matrix"):
+            continue
+        qs = [qindex[q] for q in ins.qubits]
+        U = np.zeros(16, dtype=np.complex128)
+        M = np.asarray(op.to_matrix(), dtype=np.complex128).reshape(-1)
+        U[:M.size] = M
+        if len(qs) == 1:
+            kinds.append(1); q0s.append(qs[0]); q1s.append(-1)
+        elif len(qs) == 2:
+            kinds.append(2); q0s.append(qs[0]); q1s.append(qs[1])
+        else:
+            raise ValueError(f"oracle handles 1- and 2-qubit gates, got {len(qs)}")
+        mats.append(U)
+    if psi0 is None:
+        psi = np.zeros(1 << n, dtype=dtype)
+        psi[0] = 1.0
+    else:
+        psi = np.array(psi0, dtype=dtype)
+    if not kinds:
+        return psi
+    k = np.asarray(kinds, dtype=np.int32)
+    a = np.asarray(q0s, dtype=np.int32)
+    b = np.asarray(q1s, dtype=np.int32)
+    Us = np.ascontiguousarray(np.stack(mats).view(np.float64).astype(real))  # 32 reals per op
+    run(psi.ctypes.data, n, len(kinds), k.ctypes.data, a.ctypes.data, b.ctypes.data, Us.ctypes.data)
+    return psi

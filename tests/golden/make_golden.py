@@ -2,7 +2,9 @@
 
 Run in a container where the reference checkout is readable:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference [--native-calls-only]
+
+(or set QGPUSIM_REFERENCE to the checkout and omit the path).
 
 It imports ``qgpusim/transpiler/passes.py`` and ``qgpusim/backends/custom/backend.py``
 from the reference with small ``sys.modules`` stubs: Qiskit's base-pass and DAG
@@ -22,6 +24,9 @@ Outputs (all small, committed):
   states.npz        -- final statevectors of the reference executor (physical layout
                        of the last tile) for small circuits, complex128
   fusion.npz/.json  -- ``fuse_tile_ops`` results on seeded random op lists
+  native_calls.json/.npz -- every call the reference's native branch of run_custom_backend
+                       (backend.py:405-522) makes on its native extension for the state
+                       cases, in each tile mode and precision (tests/golden/ref_harness.py)
 """
 from __future__ import annotations
 
@@ -38,39 +43,7 @@ sys.path.insert(0, REPO)
 
 from frontierlabproject_b200 import circuits as C  # noqa: E402
 from frontierlabproject_b200.circuit import QuantumCircuit, circuit_to_dag  # noqa: E402
-
-
-def install_stubs():
-    qiskit = types.ModuleType("qiskit")
-    qiskit.QuantumCircuit = QuantumCircuit
-    transpiler = types.ModuleType("qiskit.transpiler")
-    basepasses = types.ModuleType("qiskit.transpiler.basepasses")
-
-    class TransformationPass:
-        def __init__(self):
-            self.property_set = {}
-
-    basepasses.TransformationPass = TransformationPass
-    basepasses.AnalysisPass = TransformationPass
-    dagmod = types.ModuleType("qiskit.dagcircuit")
-    dagmod.DAGCircuit = object
-    dagmod.DAGOpNode = object
-    for name, mod in [("qiskit", qiskit), ("qiskit.transpiler", transpiler),
-                      ("qiskit.transpiler.basepasses", basepasses), ("qiskit.dagcircuit", dagmod)]:
-        sys.modules[name] = mod
-
-    cupy = types.ModuleType("cupy")
-    for attr in ("complex64", "complex128", "uint64", "int64", "asarray", "matmul", "zeros", "arange",
-                 "ndarray"):
-        setattr(cupy, attr, getattr(np, attr))
-    cupy.asnumpy = np.asarray
-
-    class _Pool:
-        def free_all_blocks(self):
-            pass
-
-    cupy.get_default_memory_pool = lambda: _Pool()
-    sys.modules["cupy"] = cupy
+from tests.golden.ref_harness import install_stubs, record_native_calls, save_trace  # noqa: E402
 
 
 def scatter_permute(psi, layout_old, layout_new):
@@ -138,7 +111,18 @@ def u_layers(n, depth, seed):
     return qc
 
 
-def main(ref_root):
+NATIVE_CALL_CASES = ["random_layered_n10_d6_s1_nL6", "reference_random_n10_d4_s42_nL6", "reference_ghz_n9_nL4",
+                     "reference_qft_n8_nL5", "qft_swaps_n9_nL5", "hea_n8_L3_nL5",
+                     "random_layered_n8_d4_s5_save_nL6"]
+
+
+def native_call_fixtures(ref_root, sched_cases):
+    traces = record_native_calls(ref_root, {k: sched_cases[k] for k in NATIVE_CALL_CASES})
+    save_trace(traces, os.path.join(HERE, "native_calls.json"), os.path.join(HERE, "native_calls.npz"))
+    print(f"native calls: {len(traces)} traces")
+
+
+def main(ref_root, native_calls_only=False):
     install_stubs()
     sys.path.insert(0, ref_root)
     import importlib
@@ -181,6 +165,9 @@ def main(ref_root):
     save_case.cx(0, 7)
     sched_cases["random_layered_n8_d4_s5_save_nL6"] = (save_case, 6)
 
+    if native_calls_only:
+        native_call_fixtures(ref_root, sched_cases)
+        return
     schedules = {}
     for name, (qc, nL) in sched_cases.items():
         plan = ref_plan(qc, nL)
@@ -234,8 +221,13 @@ def main(ref_root):
     np.savez_compressed(os.path.join(HERE, "fusion.npz"), **fusion_inputs)
     with open(os.path.join(HERE, "fusion.json"), "w") as f:
         json.dump(fusion_meta, f)
+    native_call_fixtures(ref_root, sched_cases)
     print("wrote fixtures to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else os.environ.get("QGPUSIM_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py /path/to/reference [--native-calls-only] (or set QGPUSIM_REFERENCE)")
+    main(root, native_calls_only="--native-calls-only" in sys.argv)

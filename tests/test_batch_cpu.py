@@ -64,3 +64,21 @@ def test_batch_argument_errors(native_lib):
         emulate(insts, BatchShape(m=8))
     with pytest.raises(RuntimeError, match="threads must be 256 or 512"):
         emulate(insts, BatchShape(threads=100))
+
+
+def test_autotune_reads_the_persisted_cache_without_timing(tmp_path):
+    # a cache entry for this batch's size signature is used as is: no candidate is built or timed
+    import json
+    from frontierlabproject_b200 import batch as B
+    insts = B.hea_batch(5, n_range=(6, 9), l_range=(2, 3), seed=3)
+    path = str(tmp_path / "tune.json")
+    key = B._cache_key(B._signature(insts))
+    with open(path, "w") as f:
+        json.dump({key: {"m": 12, "small_max": 11, "chunk": 2, "threads": 512, "blocks_per_sm": 0}}, f)
+    B._TUNED.clear()
+    shape = B.autotune(insts, shapes=[B.BatchShape(m=99)], cache_path=path)  # m=99 would fail if built
+    assert shape == B.BatchShape(m=12, small_max=11, chunk=2, threads=512)
+    B._TUNED.clear()
+    B._store_cache(path, "other", B.BatchShape())
+    with open(path) as f:
+        assert set(json.load(f)) == {key, "other"}

@@ -69,3 +69,28 @@ def test_torch_autograd():
     E_ref, g_ref = O.adjoint_gradient(C.hea_ansatz(n, L, th), a, b)
     assert abs(E.item() - E_ref) < 1e-11
     assert np.allclose(t.grad.numpy(), 2.0 * g_ref, atol=1e-10)
+
+
+def test_config3_full_size_c64_vs_c128_and_finite_differences():
+    # the benchmark workload itself: n = 24, L = 20 (960 parameters, 1440 gates), complex64
+    # states with FP64 accumulation (one persistent launch) against the complex128 adjoint, and
+    # the complex128 gradient against central finite differences (h = 1e-3) on 8 parameters
+    from frontierlabproject_b200.adjoint import AdjointEngine
+    n, L = 24, 20
+    pc, th, a, b = _case(n, L, 0)
+    assert pc.num_params == 960
+    eng32 = AdjointEngine(n, f32=True)
+    E32, g32 = eng32.energy_and_grad(pc, th, a, b)
+    assert eng32.method == "fused"
+    eng64 = AdjointEngine(n, f32=False)
+    E64, g64 = eng64.energy_and_grad(pc, th, a, b)
+    assert np.linalg.norm(g32 - g64) <= 1e-5 * np.linalg.norm(g64)
+    assert abs(E32 - E64) <= 1e-5 * max(1.0, abs(E64))
+    h = 1e-3
+    for k in (0, 1, 137, 480, 481, 700, 958, 959):
+        tp, tm = th.copy(), th.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (eng64.energy(pc, tp, a, b) - eng64.energy(pc, tm, a, b)) / (2 * h)
+        # central differences carry an O(h^2) truncation error: |E'''| h^2 / 6 ~ 1e-6 here
+        assert abs(fd - g64[k]) <= 1e-5 * max(1.0, abs(g64[k])), (k, fd, g64[k])

@@ -58,3 +58,36 @@ def test_batch_parameter_update_and_autotune():
     b.update(new)
     E, G = b.energies_and_grads()
     _check(new, E, G)
+
+
+def test_batch_largest_arena_instances_vs_complex128_engine():
+    # instances of 20-22 qubits stream their states from the HBM arena in planned passes; each
+    # is checked against the complex128 adjoint engine run on its own
+    from frontierlabproject_b200.adjoint import AdjointEngine
+    insts = hea_batch(5, n_range=(20, 22), l_range=(3, 5), seed=21)
+    insts += hea_batch(4, n_range=(12, 14), l_range=(4, 16), seed=22)
+    b = BatchedAdjoint(insts, BatchShape())
+    E, G = b.energies_and_grads()
+    for inst, e, g in zip(insts, E, G):
+        pc = inst.circuit
+        eng = AdjointEngine(pc.num_qubits, f32=False)
+        E_ref, g_ref = eng.energy_and_grad(pc, inst.theta, inst.a, inst.b)
+        assert abs(e - E_ref) <= 1e-5 * max(1.0, abs(E_ref))
+        assert np.linalg.norm(g - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+
+
+def test_autotune_cache_persists(tmp_path):
+    import json
+    from frontierlabproject_b200 import batch as B
+    insts = hea_batch(6, n_range=(8, 12), l_range=(2, 3), seed=30)
+    path = str(tmp_path / "tune.json")
+    B._TUNED.clear()
+    s1 = autotune(insts, shapes=[BatchShape(), BatchShape(m=12, small_max=10, chunk=2)], reps=1,
+                  cache_path=path)
+    with open(path) as f:
+        d = json.load(f)
+    assert len(d) == 1
+    B._TUNED.clear()
+    # a new process (empty in-memory cache) reads the file: no candidate is timed again
+    s2 = autotune(insts, shapes=[], reps=1, cache_path=path)
+    assert s2 == s1

@@ -146,3 +146,43 @@ def test_jit_teams_equal_single_team_bitwise(n):
     assert sv.get_config()["jit_blocks"] == 3
     np.testing.assert_array_equal(psi3.view(np.uint32), psi2.view(np.uint32))
     assert abs(np.vdot(psi3.astype(np.complex128), psi3).real - 1.0) <= 1e-4
+
+
+_DISK_PROBE = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, ".")
+from frontierlabproject_b200 import circuits as C
+from frontierlabproject_b200.backend import run_custom_backend
+from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
+from frontierlabproject_b200.transpiler import tile_circuit
+qc = C.random_layered(20, 6, 9)
+_, plan = tile_circuit(qc, 14)
+sv = StatevectorF32(20)
+sv.set_config(jit=1)
+psi, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv)
+st = sv.stats()
+print(json.dumps({"modules": st["jit_modules"], "hits": st["jit_disk_hits"],
+                  "sum": [float(np.real(psi).sum()), float(np.imag(psi).sum())]}))
+"""
+
+
+@pytest.mark.gpu
+def test_jit_disk_cache_across_processes(tmp_path):
+    # a second process finds every kernel module of the same program on disk and gets the same state
+    import json
+    import os
+    import subprocess
+    import sys
+    from tests.conftest import REPO
+    env = dict(os.environ, QSIM_JIT_CACHE=str(tmp_path / "jit"))
+    outs = []
+    for _ in range(2):
+        r = subprocess.run([sys.executable, "-c", _DISK_PROBE], cwd=REPO, env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    assert outs[0]["modules"] >= 1 and outs[0]["hits"] == 0
+    assert outs[1]["hits"] == outs[1]["modules"] == outs[0]["modules"]
+    assert outs[1]["sum"] == outs[0]["sum"]
+    assert any(p.endswith(".cubin") for p in os.listdir(tmp_path / "jit"))
