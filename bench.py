@@ -110,15 +110,15 @@ def build_workload(n, depth, nl, seed):
 
 
 def prepared_tiles(qc, plan, np_dtype):
-    """Per tile: (layout, fused op batch) -- the executor inputs, built once."""
-    from frontierlabproject_b200.backend import fuse_tile_ops, tile_ops_for
-    from frontierlabproject_b200.qgpusim_cuda import _OpBatch
+    """Per tile: (layout, fused op batch) -- the executor inputs, built once, as
+    run_custom_backend builds them (native preparation)."""
+    from frontierlabproject_b200.backend import prepare_tile_ops
     qmap = {q: qc.find_bit(q).index for q in qc.qubits}
     code = 0 if np_dtype == np.complex64 else 1
     out = []
     for t in plan:
-        ops = fuse_tile_ops(tile_ops_for(t, qmap, np_dtype))
-        out.append((list(t.layout), _OpBatch(ops, code) if ops else None))
+        batch, _ = prepare_tile_ops(t, qmap, code, True)
+        out.append((list(t.layout), batch if len(batch) else None))
     return out
 
 

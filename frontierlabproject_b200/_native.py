@@ -23,6 +23,12 @@ QS_ERR_INVALID = -1
 QS_ERR_CUDA = -2
 QS_ERR_DEVICE = -3
 
+# gate ids of qs_prepare_ops / qs_gate_matrix (include/qsim_b200.h)
+GATE_IDS = {"id": 1, "h": 2, "x": 3, "y": 4, "z": 5, "s": 6, "sdg": 7, "t": 8, "tdg": 9, "sx": 10, "rx": 11,
+            "ry": 12, "rz": 13, "p": 14, "u": 15, "cx": 32, "cy": 33, "cz": 34, "cp": 35, "crz": 36, "swap": 37,
+            "rzz": 38}
+QS_GATE_MATRIX = 0
+
 # qs_op {int kind, q0, q1, u_on_device; const void* U}
 OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
                      "formats": ["<i4", "<i4", "<i4", "<i4", "<u8"],
@@ -83,6 +89,9 @@ _SIGS = {
     "qs_plan_info": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), POINTER(c_int)],
     "qs_lqr_flat_tiling": [c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p],
     "qs_fuse_ops": [c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p],
+    "qs_gate_matrix": [c_int, c_void_p, c_void_p, POINTER(c_int)],
+    "qs_prepare_ops": [c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                       c_void_p],
     "qs_plan_emulate": [c_int, c_int, c_void_p, c_int, POINTER(QsConfig), c_void_p],
     "qs_perm_emulate": [c_int, c_int, c_void_p, POINTER(QsConfig), c_void_p, POINTER(c_int)],
     "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), c_void_p, c_int],

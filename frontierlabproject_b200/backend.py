@@ -22,6 +22,9 @@ from typing import List, Optional
 
 import numpy as np
 
+from ctypes import byref, c_int
+
+from . import _native as N
 from .qgpusim_cuda import Statevector, StatevectorF32, _OpBatch
 
 MAX_CACHE_SIZE = 512
@@ -129,17 +132,84 @@ def tile_ops_for(tile, qubit_map: dict, np_dtype) -> list:
     return ops
 
 
+_NO_PARAMS = (0.0, 0.0, 0.0)
+
+
+def prepare_tile_ops(tile, qubit_map: dict, dtype_code: int, fuse: bool = True):
+    """The tile's unitary nodes as a packed ``qs_op`` batch in one native call
+    (``qs_prepare_ops``: matrices of the named gates built natively, equal entry for entry to
+    ``gates.gate_matrix``; other gates through ``get_gate_matrix_host``; fused as
+    ``fuse_tile_ops`` when ``fuse``).  Returns (batch, number of gates before fusion)."""
+    g2l = tile.global_to_local_map
+    ids, q0, q1, prm = [], [], [], []
+    custom = {}
+    gate_ids = N.GATE_IDS
+    for node in tile.gates:
+        op = node.op
+        if not hasattr(op, "to_matrix"):
+            continue
+        qa = node.qargs
+        if len(qa) == 1:
+            q0.append(g2l[qubit_map[qa[0]]])
+            q1.append(-1)
+        elif len(qa) == 2:
+            q0.append(g2l[qubit_map[qa[0]]])
+            q1.append(g2l[qubit_map[qa[1]]])
+        else:
+            raise RuntimeError(f"gate {op.name} on {len(qa)} qubits is not supported (1- and 2-qubit gates only)")
+        gid = gate_ids.get(op.name) if getattr(op, "_matrix", None) is None else None
+        ps = getattr(op, "params", ())
+        pv = None
+        if gid is not None and len(ps) <= 3:
+            try:
+                pv = (float(ps[0]) if len(ps) > 0 else 0.0, float(ps[1]) if len(ps) > 1 else 0.0,
+                      float(ps[2]) if len(ps) > 2 else 0.0)
+            except (TypeError, ValueError):
+                pv = None  # symbolic parameters: the gate's own matrix
+        if pv is None:
+            custom[len(ids)] = get_gate_matrix_host(op, np.complex128)
+            ids.append(N.QS_GATE_MATRIX)
+            prm.append(_NO_PARAMS)
+        else:
+            ids.append(gid)
+            prm.append(pv)
+    n = len(ids)
+    batch = _OpBatch([], dtype_code)
+    if n == 0:
+        return batch, 0
+    cust = None
+    if custom:
+        cust = np.zeros((n, 32), dtype=np.float64)
+        for i, m in custom.items():
+            flat = np.ascontiguousarray(m, dtype=np.complex128).reshape(-1).view(np.float64)
+            cust[i, :flat.size] = flat
+    ida = np.asarray(ids, dtype=np.int32)
+    q0a = np.asarray(q0, dtype=np.int32)
+    q1a = np.asarray(q1, dtype=np.int32)
+    pa = np.asarray(prm, dtype=np.float64)
+    out = np.zeros(n, dtype=N.OP_DTYPE)
+    mats = np.empty(16 * n, dtype=np.complex64 if dtype_code == N.QS_C64 else np.complex128)
+    nout = c_int()
+    N.call("qs_prepare_ops", dtype_code, n, ida.ctypes.data, pa.ctypes.data, q0a.ctypes.data, q1a.ctypes.data,
+           cust.ctypes.data if cust is not None else None, 1 if fuse else 0, out.ctypes.data, mats.ctypes.data,
+           byref(nout))
+    batch.arr = out[:nout.value]
+    batch._keep = [mats]
+    return batch, n
+
+
 def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional[int] = None,
                        use_float32: bool = False, use_cuda_graphs: bool = True, tile_mode: str = "cooperative",
                        enable_fusion: bool = True, logical_order: bool = False, sv=None, out: np.ndarray = None,
-                       native_fusion: bool = False):
+                       native_fusion: bool = False, native_prep: bool = True):
     """Simulate ``qc`` along ``tile_plan``; returns (statevector ndarray, metrics).
 
     ``sv`` may be an existing Statevector/StatevectorF32 of the right size, reset to
     |0...0> here (avoids re-allocating HBM between runs); ``out`` an existing host array
-    (e.g. pinned) that receives the result; ``native_fusion`` packs each tile's ops and fuses
-    them in the native library (``qs_fuse_ops``, the same fusion) instead of the Python loop
-    (host matrices only; device matrices keep the Python path).
+    (e.g. pinned) that receives the result.  ``native_prep`` (default) prepares each tile's op
+    list in one native call (gate matrices, fusion and packing, ``prepare_tile_ops``); with
+    ``native_prep=False`` the per-gate Python path of the reference runs (``tile_ops_for``,
+    ``GATE_CACHE``, ``fuse_tile_ops``), and ``native_fusion`` then fuses its packed ops natively.
     """
     if tile_mode not in ("cooperative", "graphed", "sequential"):
         raise ValueError(f"unknown tile_mode: {tile_mode}")
@@ -168,13 +238,18 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
             num_reorders += 1
             layout = list(tile.layout)
         t0 = time.perf_counter()
-        ops = tile_ops_for(tile, qubit_map, np_dtype)
-        num_gates += len(ops)
-        if ops:
-            if enable_fusion and native_fusion and all(isinstance(o[-1], np.ndarray) for o in ops):
-                ops = _OpBatch(ops, 0 if np_dtype == np.complex64 else 1).fused()
-            elif enable_fusion:
-                ops = fuse_tile_ops(ops)
+        if native_prep:
+            ops, ng = prepare_tile_ops(tile, qubit_map, 0 if np_dtype == np.complex64 else 1, enable_fusion)
+            num_gates += ng
+        else:
+            ops = tile_ops_for(tile, qubit_map, np_dtype)
+            num_gates += len(ops)
+            if ops:
+                if enable_fusion and native_fusion and all(isinstance(o[-1], np.ndarray) for o in ops):
+                    ops = _OpBatch(ops, 0 if np_dtype == np.complex64 else 1).fused()
+                elif enable_fusion:
+                    ops = fuse_tile_ops(ops)
+        if len(ops):
             num_fused_ops += len(ops)
             if tile_mode == "cooperative":
                 sv.apply_tile_cooperative(ops)

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libqsim_b200.so")
 SOURCES = ["kern_pass.cu", "kern_gate.cu", "kern_adjoint.cu", "kern_batch.cu", "kern_dense_tc.cu", "kern_sample.cu",
-           "state.cu", "plan.cpp", "jit.cpp", "batch.cpp", "lqr.cpp", "fuse.cpp"]
+           "state.cu", "plan.cpp", "jit.cpp", "batch.cpp", "lqr.cpp", "fuse.cpp", "prep.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -192,6 +192,37 @@ class _StatevectorBase:
     def reset(self) -> None:
         N.call("qs_reset", self._h)
 
+    # -- checkpoint / resume (the reference has only to_numpy / from_numpy, bindings.cpp:547-574) --
+    def save(self, path: str, layout: Sequence[int] = None) -> None:
+        """Write the amplitudes (current layout, the state's precision) and ``layout``
+        (layout[p] = circuit qubit at bit position p; default identity) to ``path`` (.npz), so a
+        run can resume from the same tile of its schedule."""
+        n = self.num_qubits
+        lay = np.arange(n, dtype=np.int32) if layout is None else np.asarray(layout, dtype=np.int32)
+        if lay.shape != (n,) or sorted(lay.tolist()) != list(range(n)):
+            raise RuntimeError("layout must be a permutation of range(num_qubits)")
+        np.savez(path, psi=self.to_numpy(), layout=lay, num_qubits=np.int32(n),
+                 dtype=np.array(np.dtype(self._np_dtype).str))
+
+    def restore(self, path: str) -> List[int]:
+        """Load a checkpoint written by ``save`` into this state (same size and precision);
+        returns its layout."""
+        with np.load(path) as z:
+            psi, lay, n = z["psi"], z["layout"], int(z["num_qubits"])
+            dt = str(z["dtype"])
+        if n != self.num_qubits or np.dtype(dt) != np.dtype(self._np_dtype):
+            raise RuntimeError("checkpoint does not match the state's size / precision")
+        self.from_numpy(psi)
+        return [int(x) for x in lay]
+
+    @classmethod
+    def load(cls, path: str):
+        """A new state of this class from a checkpoint: (state, layout)."""
+        with np.load(path) as z:
+            n = int(z["num_qubits"])
+        sv = cls(n)
+        return sv, sv.restore(path)
+
     def synchronize(self) -> None:
         N.call("qs_synchronize", self._h)
 

@@ -239,6 +239,46 @@ QS_API int qs_lqr_flat_tiling(int num_qubits, int nL, const unsigned long long* 
  * dtype); *nout = fused count.  Device matrices are rejected (fuse those on the caller side). */
 QS_API int qs_fuse_ops(int dtype, const qs_op* in, int nin, qs_op* out, void* mats, int* nout);
 
+/* Gate ids of qs_prepare_ops / qs_gate_matrix: the named gates of the reference's circuits
+ * (qiskit names), QS_GATE_MATRIX = a caller-supplied matrix. */
+#define QS_GATE_MATRIX 0
+#define QS_GATE_ID 1
+#define QS_GATE_H 2
+#define QS_GATE_X 3
+#define QS_GATE_Y 4
+#define QS_GATE_Z 5
+#define QS_GATE_S 6
+#define QS_GATE_SDG 7
+#define QS_GATE_T 8
+#define QS_GATE_TDG 9
+#define QS_GATE_SX 10
+#define QS_GATE_RX 11
+#define QS_GATE_RY 12
+#define QS_GATE_RZ 13
+#define QS_GATE_P 14
+#define QS_GATE_U 15
+#define QS_GATE_CX 32
+#define QS_GATE_CY 33
+#define QS_GATE_CZ 34
+#define QS_GATE_CP 35
+#define QS_GATE_CRZ 36
+#define QS_GATE_SWAP 37
+#define QS_GATE_RZZ 38
+
+/* Matrix of a named gate (host only; replaces op.to_matrix() behind the reference's gate cache,
+ * qgpusim/backends/custom/backend.py:37-76): params[0..2] its angles; out receives 4 or 16
+ * complex128 entries (row-major, index b_q0 + 2*b_q1), *arity 1 or 2. */
+QS_API int qs_gate_matrix(int gate_id, const double* params, double* out, int* arity);
+/* A tile's op list prepared in one call (host only; replaces the per-gate loop of the
+ * reference's native branch, backend.py:432-451, its matrix cache and fuse_tile_ops,
+ * backend.py:16-200): gate i is gate_id[i] with params[3i..3i+2] on layout positions q0[i]
+ * (and q1[i] >= 0 for two-qubit gates; -1 otherwise); QS_GATE_MATRIX gates read 4 or 16
+ * complex128 entries at custom + 32 i (doubles).  fuse != 0 fuses as qs_fuse_ops does.  out (room
+ * for ngates ops) receives the ops with U pointing into mats (room for 16 ngates entries of
+ * dtype); *nout = their count. */
+QS_API int qs_prepare_ops(int dtype, int ngates, const int* gate_id, const double* params, const int* q0,
+                          const int* q1, const double* custom, int fuse, qs_op* out, void* mats, int* nout);
+
 /* Planner inspection (host only, no GPU needed): plan the ops of a tile list for an
  * n-qubit state and report sweeps / phases.  ops use physical bits. */
 QS_API int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs_config* cfg,
