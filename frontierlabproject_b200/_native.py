@@ -97,6 +97,7 @@ _SIGS = {
     "qs_jit_check": [c_int, c_void_p, c_int, POINTER(QsConfig), POINTER(c_int), c_void_p, c_int],
     "qs_apply_ops_noalloc": [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p],
     "qs_apply_dense6": [c_void_p, c_void_p],
+    "qs_apply_dense": [c_void_p, c_int, c_void_p, c_void_p],
     "qs_dense6_weights": [c_void_p, c_void_p],
     "qs_sample": [c_void_p, c_ulonglong, c_ulonglong, c_void_p],
     "qs_batch_create": [c_void_p, c_int, c_void_p, POINTER(c_void_p)],

@@ -132,6 +132,69 @@ def tile_ops_for(tile, qubit_map: dict, np_dtype) -> list:
     return ops
 
 
+def _apply_on_columns(M: np.ndarray, G: np.ndarray, slots) -> None:
+    """M <- G M, G acting on block index bits ``slots`` (1 or 2 of them; G's index
+    b_slot0 + 2 b_slot1), every column of M a state of the block's qubits."""
+    dim = M.shape[0]
+    m = dim.bit_length() - 1
+    T = M.reshape((2,) * m + (dim,))  # axis m-1-j holds index bit j
+    if len(slots) == 1:
+        ax = m - 1 - slots[0]
+        Tm = np.moveaxis(T, ax, 0)
+        Tm[...] = np.tensordot(G, Tm, axes=(1, 0))
+    else:
+        a0, a1 = m - 1 - slots[0], m - 1 - slots[1]
+        Tm = np.moveaxis(T, (a1, a0), (0, 1))  # index (b_slot1, b_slot0) = G's row/col / 2, % 2
+        Tm[...] = np.tensordot(G.reshape(2, 2, 2, 2), Tm, axes=((2, 3), (0, 1)))
+
+
+def plan_dense_blocks(ops: list, k: int) -> list:
+    """Group an op list (('1q', q, U) / ('2q', q0, q1, U) in execution order) into blocks of at
+    most k qubits: a gate joins the block that holds the last gate on each of its qubits (or a
+    block that has not met them yet) while the union stays within k; otherwise it opens a new
+    block.  Blocks run in creation order, which keeps every gate after the earlier gates on its
+    qubits and moves it only across gates on other qubits.  Returns [(qubits, U)], U the
+    2^m x 2^m product of the block's gates (m <= k), index sum_j b_{qubits[j]} 2^j."""
+    if not 1 <= k <= 6:
+        raise ValueError("dense blocks hold 1 to 6 qubits")
+    blocks: list = []   # [qubit list, gate list]
+    last: dict = {}
+    for op in ops:
+        qs = [op[1]] if op[0] == "1q" else [op[1], op[2]]
+        owners = {last.get(q) for q in qs} - {None}
+        b = None
+        if len(owners) == 1:
+            cand = owners.pop()
+            if len(set(blocks[cand][0]) | set(qs)) <= k:
+                b = cand
+        elif not owners and blocks:
+            # qubits not met yet: the most recent block can take the gate (it commutes with every
+            # earlier block) when it has room
+            cand = len(blocks) - 1
+            if len(set(blocks[cand][0]) | set(qs)) <= k:
+                b = cand
+        if b is None:
+            blocks.append([[], []])
+            b = len(blocks) - 1
+        for q in qs:
+            if q not in blocks[b][0]:
+                blocks[b][0].append(q)
+            last[q] = b
+        blocks[b][1].append(op)
+    out = []
+    for qubits, gates in blocks:
+        d = 1 << len(qubits)
+        M = np.eye(d, dtype=np.complex128)
+        slot = {q: j for j, q in enumerate(qubits)}
+        for op in gates:
+            if op[0] == "1q":
+                _apply_on_columns(M, np.asarray(op[2], dtype=np.complex128), [slot[op[1]]])
+            else:
+                _apply_on_columns(M, np.asarray(op[3], dtype=np.complex128), [slot[op[1]], slot[op[2]]])
+        out.append((list(qubits), M))
+    return out
+
+
 _NO_PARAMS = (0.0, 0.0, 0.0)
 
 
@@ -201,7 +264,7 @@ def prepare_tile_ops(tile, qubit_map: dict, dtype_code: int, fuse: bool = True):
 def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional[int] = None,
                        use_float32: bool = False, use_cuda_graphs: bool = True, tile_mode: str = "cooperative",
                        enable_fusion: bool = True, logical_order: bool = False, sv=None, out: np.ndarray = None,
-                       native_fusion: bool = False, native_prep: bool = True):
+                       native_fusion: bool = False, native_prep: bool = True, dense_fusion: int = 0):
     """Simulate ``qc`` along ``tile_plan``; returns (statevector ndarray, metrics).
 
     ``sv`` may be an existing Statevector/StatevectorF32 of the right size, reset to
@@ -210,6 +273,9 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
     list in one native call (gate matrices, fusion and packing, ``prepare_tile_ops``); with
     ``native_prep=False`` the per-gate Python path of the reference runs (``tile_ops_for``,
     ``GATE_CACHE``, ``fuse_tile_ops``), and ``native_fusion`` then fuses its packed ops natively.
+    ``dense_fusion=k`` (1..6; complex64, >= 13 qubits) groups each tile's gates into blocks of at
+    most k qubits (``plan_dense_blocks``) and applies every block as one dense unitary on the
+    tensor cores (``apply_dense_block``: one sweep per block) instead of the pass executor.
     """
     if tile_mode not in ("cooperative", "graphed", "sequential"):
         raise ValueError(f"unknown tile_mode: {tile_mode}")
@@ -219,7 +285,9 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
     t_start = time.perf_counter()
     num_tiles = len(tile_plan)
     num_reorders = num_gates = num_fused_ops = 0
-    num_kernel_launches = num_graph_replays = 0
+    num_kernel_launches = num_graph_replays = num_dense_blocks = 0
+    if dense_fusion and not use_float32:
+        raise RuntimeError("dense_fusion runs complex64 states (use_float32=True)")
     t_perm = t_apply = 0.0
 
     if sv is None:
@@ -238,6 +306,17 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
             num_reorders += 1
             layout = list(tile.layout)
         t0 = time.perf_counter()
+        if dense_fusion:
+            ops = tile_ops_for(tile, qubit_map, np.complex128)
+            num_gates += len(ops)
+            blocks = plan_dense_blocks(ops, dense_fusion)
+            num_fused_ops += len(blocks)
+            num_dense_blocks += len(blocks)
+            for qs, U in blocks:
+                sv.apply_dense_block(qs, U)
+            num_kernel_launches += len(blocks)
+            t_apply += time.perf_counter() - t0
+            continue
         if native_prep:
             ops, ng = prepare_tile_ops(tile, qubit_map, 0 if np_dtype == np.complex64 else 1, enable_fusion)
             num_gates += ng
@@ -319,5 +398,6 @@ def run_custom_backend(qc, tile_plan, task: str = "statevector", shots: Optional
         "hbm_bytes_executed": (st["sweeps"] + st["gate_sweeps"]) * sweep_bytes,
         "t_sample_s": t_sample,
         "counts": counts,
+        "dense_blocks": num_dense_blocks,
     }
     return result, metrics

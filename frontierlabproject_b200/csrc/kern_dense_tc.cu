@@ -233,7 +233,203 @@ dense6_tc_pipe_kernel(float2* __restrict__ psi, uint64_t ncols, const uint4* __r
   }
 }
 
+// ---- six arbitrary positions B: a tile is 2^13 amplitudes over T = B + the 7 lowest other bits ----
+// Local index l (13 bits over T ascending) -> row (its bits outside B, 0..127) and j (its bits in
+// B, 0..63).  T holds physical bits 0..6 (every bit below 7 is in B or among the 7 lowest others),
+// so 128 consecutive l are 1 KiB of contiguous memory: lane-consecutive 8-byte copies coalesce.
+// Per amplitude, the global offset and the staging byte (row * 512 + swizzled 16-byte chunk of j)
+// are XOR-linear in l, so each is tab_lo[l & 127] ^ tab_hi[l >> 7] (tables in the weights buffer).
+struct GatherTabs {
+  uint64_t src_lo[128];  // deposit(l, T) for l < 128
+  uint64_t src_hi[64];   // deposit(l << 7, T)
+  uint32_t dst_lo[128];  // staging byte of l < 128
+  uint32_t dst_hi[64];   // staging byte of l << 7
+  int32_t upos[64];      // physical bits outside T, ascending (the tile index's bits)
+  int32_t nu;
+  int32_t pad[3];
+};
+
+__device__ __forceinline__ void cp_async8_tc(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+
+__global__ void __launch_bounds__(128, 1)
+dense6_tc_gather_kernel(float2* __restrict__ psi, uint64_t ntiles, const uint4* __restrict__ wops,
+                        const GatherTabs* __restrict__ tabs, unsigned* err, uint64_t limit_ns) {
+  extern __shared__ __align__(1024) unsigned char smem_g[];
+  __shared__ __align__(8) uint64_t s_mb;
+  __shared__ uint32_t s_tm;
+  __shared__ int s_okg;
+  __shared__ uint64_t s_hi[64];
+  __shared__ uint32_t s_dhi[64];
+  const int t = threadIdx.x, warp = t >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem_g);
+  const uint32_t w_hi = sbase, w_lo = sbase + kOp, x_hi = sbase + 2 * kOp, x_lo = x_hi + kOp;
+  const uint32_t stg = sbase + 4 * kOp;
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mb);
+  const uint64_t my_src = tabs->src_lo[t];
+  const uint32_t my_dst = tabs->dst_lo[t];
+  const int nu = tabs->nu;
+
+  for (uint32_t i = t; i < 2 * kOp / 16; i += 128) reinterpret_cast<uint4*>(smem_g)[i] = wops[i];
+  if (t < 64) {
+    s_hi[t] = tabs->src_hi[t];
+    s_dhi[t] = tabs->dst_hi[t];
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&s_tm);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(128)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  auto base_of = [&](uint64_t tile) {
+    uint64_t b = 0;
+    for (int k = 0; k < nu; ++k)
+      if ((tile >> k) & 1ull) b |= 1ull << tabs->upos[k];
+    return b;
+  };
+  // amplitude l = 128 i + t of the tile: lanes take consecutive l (coalesced)
+  auto stage = [&](uint64_t tile) {
+    const uint64_t b = base_of(tile) | my_src;
+    for (int i = 0; i < 64; ++i) cp_async8_tc(stg + (my_dst ^ s_dhi[i]), psi + (b | s_hi[i]));
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  uint64_t tile = blockIdx.x;
+  if (tile < ntiles) stage(tile);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tm;
+  uint32_t phase = 0;
+
+  for (; tile < ntiles; tile += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const unsigned char* sp = smem_g + 4 * kOp;
+#pragma unroll 4
+    for (int j = 0; j < 16; ++j) {
+      const float4 v0 = *reinterpret_cast<const float4*>(sp + stage_off(t, 2 * j));
+      const float4 v1 = *reinterpret_cast<const float4*>(sp + stage_off(t, 2 * j + 1));
+      uint4 h, l;
+      split2(v0.x, v0.y, h.x, l.x);
+      split2(v0.z, v0.w, h.y, l.y);
+      split2(v1.x, v1.y, h.z, l.z);
+      split2(v1.z, v1.w, h.w, l.w);
+      const uint32_t off = canon(t, j);
+      asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(x_hi + off), "r"(h.x), "r"(h.y), "r"(h.z),
+                   "r"(h.w) : "memory");
+      asm volatile("st.shared.v4.b32 [%0], {%1,%2,%3,%4};" ::"r"(x_lo + off), "r"(l.x), "r"(l.y), "r"(l.z),
+                   "r"(l.w) : "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    const uint64_t next = tile + gridDim.x;
+    const uint64_t cur_base = base_of(tile) | my_src;
+    if (next < ntiles) stage(next);
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t ko = (uint32_t)k * 256u;
+        umma(tmem, sdesc(x_hi + ko), sdesc(w_hi + ko), k > 0 ? 1u : 0u);
+        umma(tmem, sdesc(x_hi + ko), sdesc(w_lo + ko), 1u);
+        umma(tmem, sdesc(x_lo + ko), sdesc(w_hi + ko), 1u);
+      }
+      umma_commit(mbar);
+      s_okg = mbar_wait(mbar, phase, limit_ns) ? 1 : 0;
+      if (!s_okg) atomicExch(err, (unsigned)DERR_BARRIER_TIMEOUT);
+    }
+    phase ^= 1u;
+    __syncthreads();
+    if (!s_okg) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    unsigned char* op = smem_g + 2 * kOp;
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t r[32];
+      TC_LD32(lane_addr + (uint32_t)(q * 32), r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        *reinterpret_cast<uint4*>(op + stage_off(t, 8 * q + e)) =
+            make_uint4(r[4 * e], r[4 * e + 1], r[4 * e + 2], r[4 * e + 3]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    // scattered 8-byte stores, lane-consecutive amplitudes (coalesced)
+    for (int i = 0; i < 64; ++i)
+      psi[cur_base | s_hi[i]] = *reinterpret_cast<const float2*>(op + (my_dst ^ s_dhi[i]));
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128) : "memory");
+  }
+}
+
 }  // namespace
+
+size_t dense6_gather_bytes() { return sizeof(GatherTabs); }
+
+// Tables of the gather kernel for the six physical bits B (ascending).  Returns false when the
+// state is too small (fewer than 13 bits).
+bool dense6_gather_tables(int n, const int* B, uint8_t* out) {
+  if (n < 13) return false;
+  GatherTabs g;
+  std::memset(&g, 0, sizeof(g));
+  bool inB[64] = {};
+  for (int q = 0; q < 6; ++q) inB[B[q]] = true;
+  int T[13], nt = 0, other = 0;
+  for (int p = 0; p < n; ++p) {
+    if (inB[p]) T[nt++] = p;
+    else if (other < 7) { T[nt++] = p; ++other; }
+    else g.upos[g.nu++] = p;
+  }
+  // within T (ascending): which bits are B (j bits, in order) and which are row bits
+  auto split = [&](uint32_t l, uint64_t* phys, uint32_t* byte) {
+    uint64_t ph = 0;
+    uint32_t row = 0, j = 0;
+    int jr = 0, rr = 0;
+    for (int b = 0; b < 13; ++b) {
+      const uint32_t v = (l >> b) & 1u;
+      if (v) ph |= 1ull << T[b];
+      if (inB[T[b]]) j |= v << jr++;
+      else row |= v << rr++;
+    }
+    *phys = ph;
+    *byte = row * 512u + ((((j >> 1) ^ (row & 7u)) & 31u) << 4) + ((j & 1u) << 3);
+  };
+  for (uint32_t l = 0; l < 128; ++l) split(l, &g.src_lo[l], &g.dst_lo[l]);
+  for (uint32_t i = 0; i < 64; ++i) split(i << 7, &g.src_hi[i], &g.dst_hi[i]);
+  std::memcpy(out, &g, sizeof(g));
+  return true;
+}
+
+cudaError_t launch_dense6_tc_gather(void* psi, int n, const void* d_weights, const void* d_tabs, unsigned* err,
+                                    uint64_t limit_ns, cudaStream_t s) {
+  if (n < 13) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(dense6_tc_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSmemPipe);
+  if (e != cudaSuccess) return e;
+  const uint64_t tiles = 1ull << (n - 13);
+  uint64_t grid = (uint64_t)device_sm_count();
+  if (grid > tiles) grid = tiles;
+  dense6_tc_gather_kernel<<<(unsigned)grid, 128, kSmemPipe, s>>>(reinterpret_cast<float2*>(psi), tiles,
+                                                                 reinterpret_cast<const uint4*>(d_weights),
+                                                                 reinterpret_cast<const GatherTabs*>(d_tabs), err,
+                                                                 limit_ns);
+  return cudaGetLastError();
+}
 
 size_t dense6_weight_bytes() { return 2 * kOp; }
 

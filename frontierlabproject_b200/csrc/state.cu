@@ -723,10 +723,65 @@ int qs_apply_dense6(qs_state* s, const double* U) {
     for (int i = 0; i < 4096; ++i) u[i] = cplx(U[2 * i], U[2 * i + 1]);
     std::vector<uint8_t> w(dense6_weight_bytes());
     dense6_prepare_weights(u.data(), w.data());
-    if (!s->d_dense) CK(dev_malloc(&s->d_dense, w.size()));
+    if (!s->d_dense) CK(dev_malloc(&s->d_dense, dense6_weight_bytes() + dense6_gather_bytes()));
     // pageable source: staged before the call returns, copied in stream order
     CK(cudaMemcpyAsync(s->d_dense, w.data(), w.size(), cudaMemcpyHostToDevice, s->stream));
     CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, s->wait_limit_ns, s->stream));
+    s->st.launches += 1;
+    s->st.gate_sweeps += 1;
+  });
+}
+
+int qs_apply_dense(qs_state* s, int k, const int* qubits, const double* U) {
+  return guard([&] {
+    if (!s || !qubits || !U) throw InvalidArg{"null argument"};
+    if (s->dtype != 0) throw InvalidArg{"apply_dense: complex64 states only"};
+    if (s->n < 13) throw InvalidArg{"apply_dense: needs at least 13 qubits"};
+    if (k < 1 || k > 6) throw InvalidArg{"apply_dense: 1 to 6 qubits"};
+    std::vector<int> bphys(k);
+    std::vector<char> used(s->n, 0);
+    for (int j = 0; j < k; ++j) {
+      if (qubits[j] < 0 || qubits[j] >= s->n) throw InvalidArg{"apply_dense: invalid qubit"};
+      bphys[j] = s->pos2bit[qubits[j]];
+      if (used[bphys[j]]++) throw InvalidArg{"apply_dense: qubits must be distinct"};
+    }
+    // the six physical bits of the kernel: the block's, then the lowest free ones (identity there)
+    std::vector<int> b6 = bphys;
+    for (int p = 0; (int)b6.size() < 6; ++p)
+      if (!used[p]) { b6.push_back(p); used[p] = 1; }
+    std::sort(b6.begin(), b6.end());
+    int slot[6];  // kernel index bit of block qubit j
+    for (int j = 0; j < k; ++j) slot[j] = (int)(std::find(b6.begin(), b6.end(), bphys[j]) - b6.begin());
+    int fmask = 63;
+    for (int j = 0; j < k; ++j) fmask &= ~(1 << slot[j]);
+    const int d = 1 << k;
+    std::vector<cplx> w(4096, cplx(0.0, 0.0));
+    auto compress = [&](int r) {
+      int v = 0;
+      for (int j = 0; j < k; ++j) v |= ((r >> slot[j]) & 1) << j;
+      return v;
+    };
+    for (int r = 0; r < 64; ++r)
+      for (int c = 0; c < 64; ++c)
+        if ((r & fmask) == (c & fmask)) {
+          const int a = compress(r), b = compress(c);
+          w[r * 64 + c] = cplx(U[2 * (a * d + b)], U[2 * (a * d + b) + 1]);
+        }
+    s->flush();  // queued gates run first (their bits are physical: no data movement needed)
+    const size_t wbytes = dense6_weight_bytes(), tbytes = dense6_gather_bytes();
+    std::vector<uint8_t> buf(wbytes + tbytes);
+    dense6_prepare_weights(w.data(), buf.data());
+    const bool low6 = b6 == std::vector<int>{0, 1, 2, 3, 4, 5};
+    if (!low6 && !dense6_gather_tables(s->n, b6.data(), buf.data() + wbytes))
+      throw InvalidArg{"apply_dense: needs at least 13 qubits"};
+    if (!s->d_dense) CK(dev_malloc(&s->d_dense, wbytes + tbytes));
+    CK(cudaMemcpyAsync(s->d_dense, buf.data(), buf.size(), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));  // the pageable source is read before it goes out of scope
+    if (low6)
+      CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, s->wait_limit_ns, s->stream));
+    else
+      CK(launch_dense6_tc_gather(s->psi, s->n, s->d_dense, (const uint8_t*)s->d_dense + wbytes, s->d_ctl + 2,
+                                 s->wait_limit_ns, s->stream));
     s->st.launches += 1;
     s->st.gate_sweeps += 1;
   });

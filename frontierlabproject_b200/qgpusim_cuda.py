@@ -272,6 +272,17 @@ class _StatevectorBase:
         N.call("qs_apply_dense6", self._h, U.ctypes.data)
         self.permute(moved, ident)
 
+    def apply_dense_block(self, qubits: Sequence[int], U) -> None:
+        """Dense 2^k x 2^k unitary (k = len(qubits) <= 6) on layout positions ``qubits`` in one
+        tensor-core sweep (complex64, >= 13 qubits); row/column index sum_j b_{qubits[j]} 2^j.
+        No data moves to another layout (the kernel gathers the block's bits in place)."""
+        q = np.ascontiguousarray([int(x) for x in qubits], dtype=np.int32)
+        k = q.size
+        U = np.ascontiguousarray(U, dtype=np.complex128)
+        if U.shape != (1 << k, 1 << k):
+            raise RuntimeError(f"U must be a {1 << k}x{1 << k} matrix")
+        N.call("qs_apply_dense", self._h, int(k), q.ctypes.data, U.ctypes.data)
+
     # -- layout ------------------------------------------------------------------------
     def permute(self, layout_old: Sequence[int], layout_new: Sequence[int]) -> None:
         n = self.num_qubits

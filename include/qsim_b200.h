@@ -140,6 +140,14 @@ QS_API int qs_materialize(qs_state* s);
  * One sweep on the tensor cores (tcgen05 MMAs, operands split into BF16 high and low parts,
  * FP32 accumulation in tensor memory); queued gates run first and the layout is materialised. */
 QS_API int qs_apply_dense6(qs_state* s, const double* U);
+/* Dense 2^k x 2^k unitary (k = 1..6) on k arbitrary layout positions qubits[0..k-1] of a
+ * complex64 state of >= 13 qubits, in one tensor-core sweep (no counterpart in the reference
+ * executor: the fused k-qubit blocks of the north-star design).  U: host complex128, row-major,
+ * row/column index sum_j b_{qubits[j]} 2^j.  Applied as the 64x64 unitary U (x) I on the block's
+ * bits and the lowest other physical bits; a tile of the kernel is 2^13 amplitudes over those six
+ * bits and the seven lowest other bits (coalesced copies for any positions).  Queued gates run
+ * first; no data is moved to another layout. */
+QS_API int qs_apply_dense(qs_state* s, int k, const int* qubits, const double* U);
 /* Measurement sampling (the runner's "sampling" task, runner.py:25-27, 74; the reference's custom
  * backend has none): `shots` basis indices (layout order, bit p = position p) drawn from |psi|^2,
  * returned ascending in out (host, shots entries).  Queued gates run first.  seed selects the

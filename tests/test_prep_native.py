@@ -90,3 +90,38 @@ def test_prepare_rejects_bad_input(native_lib):
     rc = N.lib().qs_prepare_ops(0, 1, ids.ctypes.data, z.ctypes.data, a.ctypes.data, b.ctypes.data, None, 1,
                                 out.ctypes.data, mats.ctypes.data, ctypes.byref(nout))
     assert rc == N.QS_ERR_INVALID and b"arity" in N.lib().qs_last_error()
+
+
+@pytest.mark.parametrize("k", [2, 4, 5, 6])
+def test_dense_block_plan_reproduces_the_tile(k):
+    # the blocks' products, applied in order, equal the tile's gates applied one by one
+    from frontierlabproject_b200.backend import plan_dense_blocks
+    from oracle import statevector as O
+    for qc, nl in ((_mixed(10, 4), 10), (C.random_layered(9, 6, 1), 9), (_fusing_circuit(8, 3), 8)):
+        _, plan = tile_circuit(qc, nl)
+        qmap = {q: qc.find_bit(q).index for q in qc.qubits}
+        rng = np.random.default_rng(5)
+        for t in plan:
+            ops = tile_ops_for(t, qmap, np.complex128)
+            n = qc.num_qubits
+            psi = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+            want = psi.copy()
+            for op in ops:
+                if op[0] == "1q":
+                    O.apply_1q(want, op[2], op[1])
+                else:
+                    O.apply_2q(want, op[3], op[1], op[2])
+            blocks = plan_dense_blocks(ops, k)
+            assert all(len(qs) <= k for qs, _ in blocks)
+            got = psi.copy()
+            for qs, U in blocks:
+                # apply the block as a dense unitary on qubits qs (index sum_j b_qs[j] 2^j)
+                m = len(qs)
+                v = got.reshape((2,) * n)
+                axes = [n - 1 - q for q in qs][::-1]  # block index bit m-1 .. 0
+                vm = np.moveaxis(v, axes, list(range(m)))
+                sh = vm.shape
+                vm[...] = (U @ vm.reshape(1 << m, -1)).reshape(sh)
+            np.testing.assert_allclose(got, want, atol=1e-12)
+            if k >= 2:
+                assert len(blocks) <= len(ops)
