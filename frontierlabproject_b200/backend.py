@@ -150,43 +150,95 @@ def _apply_on_columns(M: np.ndarray, G: np.ndarray, slots) -> None:
 
 def plan_dense_blocks(ops: list, k: int) -> list:
     """Group an op list (('1q', q, U) / ('2q', q0, q1, U) in execution order) into blocks of at
-    most k qubits: a gate joins the block that holds the last gate on each of its qubits (or a
-    block that has not met them yet) while the union stays within k; otherwise it opens a new
-    block.  Blocks run in creation order, which keeps every gate after the earlier gates on its
-    qubits and moves it only across gates on other qubits.  Returns [(qubits, U)], U the
-    2^m x 2^m product of the block's gates (m <= k), index sum_j b_{qubits[j]} 2^j."""
+    most k qubits, run in creation order.  Every gate must stay after the earlier gates on its
+    qubits and may only move across gates on other qubits; with last[q] the block holding the
+    latest gate on q:
+
+    * a one-qubit gate waits on its qubit and is placed just before the next two-qubit gate on
+      that qubit, in that gate's block (or, at the end, in last[q]);
+    * a gate joins the later of its qubits' last blocks when the qubit union stays within k (the
+      blocks in between do not touch its other qubit, since that qubit's last block is earlier);
+    * when its qubits' last blocks b1 < b2 are both still the latest blocks of all their qubits
+      and fit together in k qubits, b1 moves into b2 (nothing between them touches b1's qubits)
+      and the gate joins the merged block;
+    * a gate on qubits no block has met joins the most recent block with room; otherwise a new
+      block opens.
+
+    Returns [(qubits, U)], U the 2^m x 2^m product of the block's gates (m <= k), row/column
+    index sum_j b_{qubits[j]} 2^j."""
     if not 1 <= k <= 6:
         raise ValueError("dense blocks hold 1 to 6 qubits")
-    blocks: list = []   # [qubit list, gate list]
+    qsets: list = []   # qubits of each block (first-touch order)
+    gates: list = []
+    alive: list = []
     last: dict = {}
-    for op in ops:
-        qs = [op[1]] if op[0] == "1q" else [op[1], op[2]]
-        owners = {last.get(q) for q in qs} - {None}
-        b = None
-        if len(owners) == 1:
-            cand = owners.pop()
-            if len(set(blocks[cand][0]) | set(qs)) <= k:
-                b = cand
-        elif not owners and blocks:
-            # qubits not met yet: the most recent block can take the gate (it commutes with every
-            # earlier block) when it has room
-            cand = len(blocks) - 1
-            if len(set(blocks[cand][0]) | set(qs)) <= k:
-                b = cand
-        if b is None:
-            blocks.append([[], []])
-            b = len(blocks) - 1
+    pending: dict = {}
+
+    def add(b, op, qs):
         for q in qs:
-            if q not in blocks[b][0]:
-                blocks[b][0].append(q)
+            if q not in qsets[b]:
+                qsets[b].append(q)
             last[q] = b
-        blocks[b][1].append(op)
+        gates[b].append(op)
+
+    def latest(b):
+        return all(last.get(q) == b for q in qsets[b])
+
+    def newest_with_room(qs):
+        for c in range(len(qsets) - 1, -1, -1):
+            if alive[c]:
+                return c if len(set(qsets[c]) | set(qs)) <= k else None
+        return None
+
+    def open_block():
+        qsets.append([])
+        gates.append([])
+        alive.append(True)
+        return len(qsets) - 1
+
+    for op in ops:
+        if op[0] == "1q":
+            pending.setdefault(op[1], []).append(op)
+            continue
+        qs = [op[1], op[2]]
+        owners = sorted({last.get(q) for q in qs} - {None})
+        b = None
+        if len(owners) == 2:
+            b1, b2 = owners
+            if len(set(qsets[b1]) | set(qsets[b2])) <= k and latest(b1) and latest(b2):
+                gates[b2] = gates[b1] + gates[b2]
+                for q in qsets[b1]:
+                    qsets[b2].append(q)
+                    last[q] = b2
+                alive[b1], gates[b1], qsets[b1] = False, [], []
+                b = b2
+        if b is None and owners and len(set(qsets[owners[-1]]) | set(qs)) <= k:
+            b = owners[-1]
+        if b is None and not owners:
+            b = newest_with_room(qs)
+        if b is None:
+            b = open_block()
+        for q in qs:
+            for g in pending.pop(q, []):
+                add(b, g, [q])
+        add(b, op, qs)
+    for q in list(pending):
+        b = last.get(q)
+        if b is None:
+            b = newest_with_room([q])
+        if b is None:
+            b = open_block()
+        for g in pending.pop(q):
+            add(b, g, [q])
     out = []
-    for qubits, gates in blocks:
+    for b in range(len(qsets)):
+        if not alive[b] or not gates[b]:
+            continue
+        qubits = qsets[b]
         d = 1 << len(qubits)
         M = np.eye(d, dtype=np.complex128)
         slot = {q: j for j, q in enumerate(qubits)}
-        for op in gates:
+        for op in gates[b]:
             if op[0] == "1q":
                 _apply_on_columns(M, np.asarray(op[2], dtype=np.complex128), [slot[op[1]]])
             else:
