@@ -440,6 +440,34 @@ def dense_fusion_bench(qc, plan, k, sv64, hbm_peak) -> dict:
                     "executor, which stays the timed path"}
 
 
+def cold_start_async_bench(args) -> dict:
+    """First call of a circuit structure this process has not compiled (the same family, next
+    seed) with jit_async: the generic pass kernel runs it while the specialised kernels compile in
+    the background; then the wait for the compile and the first specialised run."""
+    from frontierlabproject_b200.backend import run_custom_backend
+    from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
+    qc, plan, _ = build_workload(args.n, args.depth, args.nl, args.seed + 1)
+    sv = StatevectorF32(args.n)
+    sv.set_config(jit_async=1)
+    out = np.empty(1 << args.n, dtype=np.complex64)
+    t0 = time.perf_counter()
+    run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv, out=out)
+    t_first = time.perf_counter() - t0
+    pending = sv.stats()["jit_pending_flushes"]
+    t0 = time.perf_counter()
+    StatevectorF32.jit_wait()
+    t_wait = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv, out=out)
+    t_second = time.perf_counter() - t0
+    st = sv.stats()
+    sv.close()
+    return {"workload": f"random circuit n={args.n} depth={args.depth} seed {args.seed + 1} (a new structure), "
+                        "end to end through run_custom_backend",
+            "first_call_s": t_first, "generic_flushes": pending, "compile_wait_after_first_s": t_wait,
+            "second_call_s": t_second, "second_call_specialised_modules": st["jit_modules"]}
+
+
 def n33_bench(args, hbm_peak) -> dict:
     """The same circuit family at n=33 (64 GiB complex64 state), depth 100, the reference
     schedule at nL=20: device time per circuit (CUDA events), B_alg / t and the sweep count."""
@@ -537,6 +565,8 @@ def main():
     ap.add_argument("--no-fidelity", action="store_true")
     ap.add_argument("--n33", type=int, default=1, help="also time the n=33 circuit (64 GiB state)")
     ap.add_argument("--ref-units", type=int, default=16, help="reference arm: work units per step")
+    ap.add_argument("--cold-async", type=int, default=1, help="time a new circuit structure's first call with "
+                                                                "the generic kernel standing in while compiling")
     ap.add_argument("--dense-k", type=int, default=6, help="also time the circuit as fused k-qubit tensor-core "
                                                           "blocks (0: skip)")
     args = ap.parse_args()
@@ -692,6 +722,10 @@ def main():
     if args.n33 and world == 1:
         big = n33_bench(args, hbm_peak)
 
+    cold = None
+    if args.cold_async and world == 1:
+        cold = cold_start_async_bench(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         ref = CpuReference(qc, plan, choose_cpu_n(n))
@@ -718,6 +752,7 @@ def main():
                 "sweeps_per_step": sweeps_step, "reference_sweeps_per_step": len(plan) + R + 1,
                 "fidelity_err_vs_fp64": fid["fidelity_err_vs_fp64"] if fid else None, "fidelity": fid,
                 "first_call_s": first_call_s, "first_call_compile_s": first["jit_compile_ms"] / 1e3,
+                "first_call_async": cold,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                              "frac": achieved / hbm_peak, "traffic": None,
                              "traffic_note": "DRAM bytes per launch come from ncu captures of this kernel "

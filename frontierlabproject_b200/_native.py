@@ -37,14 +37,15 @@ OP_DTYPE = np.dtype({"names": ["kind", "q0", "q1", "dev", "U"],
 
 class QsConfig(ctypes.Structure):
     _fields_ = [("m", c_int), ("k", c_int), ("hill_iters", c_int), ("grid_mult", c_int), ("jit", c_int),
-                ("jit_lr", c_int), ("jit_blocks", c_int), ("jit_packed", c_int), ("wait_limit_ns", c_ulonglong)]
+                ("jit_lr", c_int), ("jit_blocks", c_int), ("jit_packed", c_int), ("wait_limit_ns", c_ulonglong),
+                ("jit_async", c_int), ("pad", c_int)]
 
 
 class QsStats(ctypes.Structure):
     _fields_ = [(name, c_ulonglong) for name in
                 ("gates", "sweeps", "perm_sweeps", "gate_sweeps", "launches", "graph_replays",
                  "graph_builds", "flushes", "permutes", "plans", "jit_compile_ms", "jit_modules",
-                 "jit_disk_hits")]
+                 "jit_disk_hits", "jit_pending_flushes")]
 
     def as_dict(self) -> dict:
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
@@ -54,6 +55,7 @@ class QsStats(ctypes.Structure):
 _SIGS = {
     "qs_version": [],
     "qs_debug_fail_alloc": [c_int],
+    "qs_jit_wait": [],
     "qs_device_count": [POINTER(c_int)],
     "qs_create": [c_int, c_int, POINTER(c_void_p)],
     "qs_destroy": [c_void_p],

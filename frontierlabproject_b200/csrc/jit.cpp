@@ -14,6 +14,7 @@
 #include <fstream>
 #include <functional>
 #include <cstring>
+#include <future>
 #include <list>
 #include <mutex>
 #include <sstream>
@@ -1112,6 +1113,51 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg_in
   g_cache.push_front(k);
   while (g_cache.size() > 8) g_cache.pop_back();
   return k;
+}
+
+namespace {
+// compiles started by jit_try_get and not yet collected, by kernel key (guarded by g_mu)
+std::unordered_map<uint64_t, std::shared_future<std::shared_ptr<JitKernels>>> g_inflight;
+}  // namespace
+
+std::shared_ptr<JitKernels> jit_try_get(const Program& prog, const JitConfig& cfg_in) {
+  std::string why;
+  if (!jit_available(&why)) throw std::runtime_error("jit: " + why);
+  const JitConfig cfg = jit_effective(prog, cfg_in);
+  const uint64_t key = jit_key(prog, cfg);
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
+    if ((*it)->key == key) {
+      auto k = *it;
+      g_cache.erase(it);
+      g_cache.push_front(k);
+      return k;
+    }
+  auto it = g_inflight.find(key);
+  if (it != g_inflight.end()) {
+    if (it->second.wait_for(std::chrono::seconds(0)) != std::future_status::ready) return nullptr;
+    auto fut = it->second;
+    g_inflight.erase(it);
+    return fut.get();  // the compiled kernels (also in the cache now), or the compile's error
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("jit: no current device");
+  Program copy = prog;
+  // the compiling thread makes the same device current (its driver calls load the modules there)
+  g_inflight.emplace(key, std::async(std::launch::async, [copy, cfg_in, dev]() {
+                            if (cudaSetDevice(dev) != cudaSuccess) throw std::runtime_error("jit: cannot set the device");
+                            return jit_get(copy, cfg_in);
+                          }).share());
+  return nullptr;
+}
+
+void jit_wait_all() {
+  std::vector<std::shared_future<std::shared_ptr<JitKernels>>> futs;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& kv : g_inflight) futs.push_back(kv.second);
+  }
+  for (auto& f : futs) f.wait();
 }
 
 cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,

@@ -57,6 +57,13 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
 // disables it), keyed by their source, the device headers, the options and NVRTC's version.
 std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg);
 
+// Non-blocking form of jit_get: the kernels when they are compiled (in memory), else nullptr
+// after starting (once per program structure) their compile on a background thread; a
+// later call returns them once that compile has finished (or throws its error).
+std::shared_ptr<JitKernels> jit_try_get(const Program& prog, const JitConfig& cfg);
+// Waits for every compile started by jit_try_get.
+void jit_wait_all();
+
 // Launch the specialised kernel of pass p (one launch per pass, no grid barrier).
 // host_coef = the program's coefficient table in host memory: the pass's range of it is
 // copied into the launch's parameter block.  smem_double = bytes of two group buffers

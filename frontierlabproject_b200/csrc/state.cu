@@ -127,6 +127,7 @@ struct qs_state {
   int jit_mode = 0;        // 0 auto (complex64, n >= 20, graphed), 1 always, -1 never
   int jit_lr = 5;          // register bits per thread of the specialised kernels
   int jit_packed = 0;      // FP32x2 arithmetic in the specialised kernels
+  int jit_async = 0;       // generic kernels stand in while a structure's specialised kernels compile
   int jit_blocks = 2;      // resident blocks per SM of the specialised kernels (single-buffered
                            // blocks that overlap each other's group loads)
   uint64_t wait_limit_ns = kBarrierLimitNs;  // bounded device waits of the pass kernel's grid
@@ -227,6 +228,27 @@ struct qs_state {
   void run_program(const Program& prog, int mode, bool use_jit = false) {
     if (prog.npass == 0) return;
     upload(prog);
+    std::shared_ptr<JitKernels> jk;
+    if (use_jit && mode != QS_MODE_COOPERATIVE) {
+      JitConfig jc;
+      jc.blocks = jit_blocks;
+      jc.packed = jit_packed != 0;
+      // while the specialised kernels of a new structure compile, the generic kernel runs the
+      // same program (it takes the plan of 5 register bits with interleaved registers)
+      const bool stand_in = jit_async != 0 && jit_lr == 5 && jit_packed == 0;
+      jk = stand_in ? jit_try_get(prog, jc) : jit_get(prog, jc);
+      if (jk) {
+        st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
+        st.jit_modules += (unsigned long long)jk->chunks;
+        st.jit_disk_hits += (unsigned long long)jk->disk_hits;
+        jk->compile_seconds = 0.0;  // counted once
+        jk->chunks = 0;
+        jk->disk_hits = 0;
+      } else {
+        st.jit_pending_flushes += 1;
+      }
+      use_jit = jk != nullptr;
+    }
     const int grid = use_jit ? 0 : grid_for_program(prog);
     if (mode == QS_MODE_COOPERATIVE) {
       CK(cudaMemsetAsync(d_ctl, 0, 2 * sizeof(unsigned), stream));
@@ -234,20 +256,7 @@ struct qs_state {
                             d_ctl + 2, wait_limit_ns, stream));
       st.launches += 1;
     } else {
-      // specialised kernels for large complex64 states (compiled once per structure)
-      std::shared_ptr<JitKernels> jk;
-      if (use_jit) {
-        JitConfig jc;
-        jc.blocks = jit_blocks;
-        jc.packed = jit_packed != 0;
-        jk = jit_get(prog, jc);
-        st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
-        st.jit_modules += (unsigned long long)jk->chunks;
-        st.jit_disk_hits += (unsigned long long)jk->disk_hits;
-        jk->compile_seconds = 0.0;  // counted once
-        jk->chunks = 0;
-        jk->disk_hits = 0;
-      }
+      // specialised kernels for large complex64 states (compiled once per structure): jk
       const uint64_t skey = jk ? jk->key : prog.structure_hash;
       const uint64_t key = skey ^ ((uint64_t)(uintptr_t)psi * 0x9E3779B97F4A7C15ull) ^
                            ((uint64_t)(uintptr_t)d_prog << 1) ^ (uint64_t)grid ^ (jk ? 0x5bd1e995ull : 0ull);
@@ -511,6 +520,10 @@ void enqueue(qs_state* s, std::vector<QOp>&& ops, int mode) {
 extern "C" {
 
 const char* qs_last_error(void) { return g_err.c_str(); }
+
+int qs_jit_wait(void) {
+  return guard([&] { jit_wait_all(); });
+}
 
 int qs_debug_fail_alloc(int k) {
   g_fail_alloc.store(k > 0 ? k : 0);
@@ -827,6 +840,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     if (c->jit_lr < 3 || c->jit_lr > 5 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
     if (c->jit_blocks < 1 || c->jit_blocks > 4) throw InvalidArg{"config: jit_blocks must be 1, 2, 3 or 4"};
     if (c->jit_packed < 0 || c->jit_packed > 1) throw InvalidArg{"config: jit_packed must be 0 or 1"};
+    if (c->jit_async < 0 || c->jit_async > 1) throw InvalidArg{"config: jit_async must be 0 or 1"};
     s->flush();
     s->cfg.m = c->m;
     s->cfg.k = c->k;
@@ -837,6 +851,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     s->jit_blocks = c->jit_blocks;
     s->jit_packed = c->jit_packed;
     s->wait_limit_ns = c->wait_limit_ns ? c->wait_limit_ns : kBarrierLimitNs;
+    s->jit_async = c->jit_async;
   });
 }
 
@@ -849,6 +864,7 @@ int qs_get_config(qs_state* s, qs_config* c) {
     c->jit_blocks = s->jit_blocks;
     c->jit_packed = s->jit_packed;
     c->wait_limit_ns = s->wait_limit_ns;
+    c->jit_async = s->jit_async;
   });
 }
 

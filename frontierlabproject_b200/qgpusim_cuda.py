@@ -355,15 +355,19 @@ class _StatevectorBase:
 
     def set_config(self, m: int = None, k: int = None, hill_iters: int = None, grid_mult: int = None,
                    jit: int = None, jit_lr: int = None, jit_blocks: int = None, jit_packed: int = None,
-                   wait_limit_ns: int = None) -> None:
+                   wait_limit_ns: int = None, jit_async: int = None) -> None:
         """Executor knobs: staged bits per sweep ``m``, always-staged low bits ``k``, planner
         effort ``hill_iters``, blocks per SM ``grid_mult``, specialised kernels ``jit``
         (0 auto, 1 always, -1 never) with ``jit_lr`` register bits per thread,
         ``jit_blocks`` geometry (1 double-buffered block per SM, 2 single-buffered blocks per
         SM, 3 one block of two teams over three buffers), ``jit_packed`` FP32x2 arithmetic and
-        ``wait_limit_ns``, the limit of the kernels' bounded device waits (0: 20 s)."""
+        ``wait_limit_ns``, the limit of the kernels' bounded device waits (0: 20 s), and
+        ``jit_async`` (1: the generic kernel runs while a new structure's specialised kernels
+        compile in the background)."""
         c = N.QsConfig()
         N.call("qs_get_config", self._h, byref(c))
+        if jit_async is not None:
+            c.jit_async = int(jit_async)
         if wait_limit_ns is not None:
             c.wait_limit_ns = int(wait_limit_ns)
         if jit is not None:
@@ -389,7 +393,12 @@ class _StatevectorBase:
         N.call("qs_get_config", self._h, byref(c))
         return {"m": c.m, "k": c.k, "hill_iters": c.hill_iters, "grid_mult": c.grid_mult, "jit": c.jit,
                 "jit_lr": c.jit_lr, "jit_blocks": c.jit_blocks, "jit_packed": c.jit_packed,
-                "wait_limit_ns": int(c.wait_limit_ns)}
+                "wait_limit_ns": int(c.wait_limit_ns), "jit_async": c.jit_async}
+
+    @staticmethod
+    def jit_wait() -> None:
+        """Wait for every background compile of specialised kernels (``jit_async``)."""
+        N.call("qs_jit_wait")
 
     def device_ptr(self) -> int:
         p = c_void_p()

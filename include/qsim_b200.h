@@ -71,6 +71,11 @@ typedef struct {
                                        completion waits); 0 = the default, 20 s.  A wait that
                                        expires sets an error word; the call that observes it
                                        returns QS_ERR_DEVICE and the state stays usable. */
+  int jit_async;  /* 1: while the specialised kernels of a new circuit structure compile (on a
+                     background thread), the generic pass kernel runs the same plan (needs
+                     jit_lr = 5 and jit_packed = 0); later flushes use the specialised kernels
+                     once they are ready.  0 (default): the first flush waits for the compile. */
+  int pad;
 } qs_config;
 
 typedef struct {
@@ -87,6 +92,7 @@ typedef struct {
   unsigned long long jit_compile_ms; /* host time spent compiling specialised kernels */
   unsigned long long jit_modules;    /* kernel modules prepared for specialised programs */
   unsigned long long jit_disk_hits;  /* of which read from the on-disk kernel cache */
+  unsigned long long jit_pending_flushes; /* flushes run by the generic kernel while compiling */
 } qs_stats;
 
 /* Library */
@@ -96,6 +102,8 @@ QS_API const char* qs_last_error(void);
  * benches/run_benchmarks.py:192-213): the k-th next device or pinned-host allocation made by
  * the library fails with a CUDA out-of-memory error and allocates nothing (k <= 0: off). */
 QS_API int qs_debug_fail_alloc(int k);
+/* Waits until every background compile of specialised kernels (qs_config.jit_async) has ended. */
+QS_API int qs_jit_wait(void);
 QS_API int qs_version(void);
 QS_API int qs_device_count(int* out);
 

@@ -186,3 +186,26 @@ def test_jit_disk_cache_across_processes(tmp_path):
     assert outs[1]["hits"] == outs[1]["modules"] == outs[0]["modules"]
     assert outs[1]["sum"] == outs[0]["sum"]
     assert any(p.endswith(".cubin") for p in os.listdir(tmp_path / "jit"))
+
+
+@pytest.mark.gpu
+def test_jit_async_generic_stand_in_then_specialised():
+    # a new structure: the first run goes through the generic kernel while the specialised
+    # kernels compile in the background; after qs_jit_wait the next run uses them; both exact
+    qc = C.random_layered(20, 8, 31)
+    _, plan = tile_circuit(qc, 14)
+    ref = O.simulate(qc)
+    sv = StatevectorF32(20)
+    sv.set_config(jit=1, jit_async=1)
+    assert sv.get_config()["jit_async"] == 1
+    psi, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv,
+                                logical_order=True)
+    st = sv.stats()
+    assert st["jit_pending_flushes"] >= 1 and st["jit_modules"] == 0
+    assert O.infidelity(ref, psi) <= 1e-5
+    StatevectorF32.jit_wait()
+    psi2, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv,
+                                 logical_order=True)
+    st = sv.stats()
+    assert st["jit_modules"] >= 1 and st["jit_pending_flushes"] == 0
+    assert O.infidelity(ref, psi2) <= 1e-5
