@@ -54,7 +54,7 @@ def test_cooperative_barrier_wait_expires_and_state_recovers():
     assert sv.get_config()["wait_limit_ns"] == 20 * 10 ** 9
     psi, _ = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="cooperative", sv=sv,
                                 logical_order=True)
-    assert O.infidelity(O.simulate(qc), psi) <= 1e-5
+    assert O.infidelity(O.simulate_c(qc), psi) <= 1e-5
 
 
 def test_batch_dependency_wait_expires_then_runs():
