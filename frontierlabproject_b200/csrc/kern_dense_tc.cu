@@ -244,15 +244,22 @@ struct GatherTabs {
   uint64_t src_hi[64];   // deposit(l << 7, T)
   uint32_t dst_lo[128];  // staging byte of l < 128
   uint32_t dst_hi[64];   // staging byte of l << 7
+  // pairs (physical bit 0 in B: amplitudes 2p and 2p + 1 are adjacent in memory and in a row):
+  uint64_t psrc_lo[128];  // deposit(2 p, T) for p < 128
+  uint64_t psrc_hi[32];   // deposit(p << 8, T)
+  uint32_t pdst_lo[128];
+  uint32_t pdst_hi[32];
   int32_t upos[64];      // physical bits outside T, ascending (the tile index's bits)
   int32_t nu;
-  int32_t pad[3];
+  int32_t pairs;         // 1: physical bit 0 is in B (16-byte copies)
+  int32_t pad[2];
 };
 
 __device__ __forceinline__ void cp_async8_tc(uint32_t dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
 }
 
+template <bool kPairs>
 __global__ void __launch_bounds__(128, 1)
 dense6_tc_gather_kernel(float2* __restrict__ psi, uint64_t ntiles, const uint4* __restrict__ wops,
                         const GatherTabs* __restrict__ tabs, unsigned* err, uint64_t limit_ns) {
@@ -267,14 +274,15 @@ dense6_tc_gather_kernel(float2* __restrict__ psi, uint64_t ntiles, const uint4* 
   const uint32_t w_hi = sbase, w_lo = sbase + kOp, x_hi = sbase + 2 * kOp, x_lo = x_hi + kOp;
   const uint32_t stg = sbase + 4 * kOp;
   const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mb);
-  const uint64_t my_src = tabs->src_lo[t];
-  const uint32_t my_dst = tabs->dst_lo[t];
+  constexpr int kItems = kPairs ? 32 : 64;  // copies per thread per tile
+  const uint64_t my_src = kPairs ? tabs->psrc_lo[t] : tabs->src_lo[t];
+  const uint32_t my_dst = kPairs ? tabs->pdst_lo[t] : tabs->dst_lo[t];
   const int nu = tabs->nu;
 
   for (uint32_t i = t; i < 2 * kOp / 16; i += 128) reinterpret_cast<uint4*>(smem_g)[i] = wops[i];
-  if (t < 64) {
-    s_hi[t] = tabs->src_hi[t];
-    s_dhi[t] = tabs->dst_hi[t];
+  if (t < kItems) {
+    s_hi[t] = kPairs ? tabs->psrc_hi[t] : tabs->src_hi[t];
+    s_dhi[t] = kPairs ? tabs->pdst_hi[t] : tabs->dst_hi[t];
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
@@ -293,10 +301,14 @@ dense6_tc_gather_kernel(float2* __restrict__ psi, uint64_t ntiles, const uint4* 
       if ((tile >> k) & 1ull) b |= 1ull << tabs->upos[k];
     return b;
   };
-  // amplitude l = 128 i + t of the tile: lanes take consecutive l (coalesced)
+  // amplitude l = 128 i + t (pair 2 (128 i + t) with kPairs) of the tile: lanes take consecutive
+  // l (coalesced)
   auto stage = [&](uint64_t tile) {
     const uint64_t b = base_of(tile) | my_src;
-    for (int i = 0; i < 64; ++i) cp_async8_tc(stg + (my_dst ^ s_dhi[i]), psi + (b | s_hi[i]));
+    for (int i = 0; i < kItems; ++i) {
+      if constexpr (kPairs) cp_async16_tc(stg + (my_dst ^ s_dhi[i]), psi + (b | s_hi[i]));
+      else cp_async8_tc(stg + (my_dst ^ s_dhi[i]), psi + (b | s_hi[i]));
+    }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   uint64_t tile = blockIdx.x;
@@ -364,9 +376,13 @@ dense6_tc_gather_kernel(float2* __restrict__ psi, uint64_t ntiles, const uint4* 
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    // scattered 8-byte stores, lane-consecutive amplitudes (coalesced)
-    for (int i = 0; i < 64; ++i)
-      psi[cur_base | s_hi[i]] = *reinterpret_cast<const float2*>(op + (my_dst ^ s_dhi[i]));
+    // scattered 8- or 16-byte stores, lane-consecutive amplitudes (coalesced)
+    for (int i = 0; i < kItems; ++i) {
+      if constexpr (kPairs)
+        *reinterpret_cast<float4*>(psi + (cur_base | s_hi[i])) = *reinterpret_cast<const float4*>(op + (my_dst ^ s_dhi[i]));
+      else
+        psi[cur_base | s_hi[i]] = *reinterpret_cast<const float2*>(op + (my_dst ^ s_dhi[i]));
+    }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -411,23 +427,25 @@ bool dense6_gather_tables(int n, const int* B, uint8_t* out) {
   };
   for (uint32_t l = 0; l < 128; ++l) split(l, &g.src_lo[l], &g.dst_lo[l]);
   for (uint32_t i = 0; i < 64; ++i) split(i << 7, &g.src_hi[i], &g.dst_hi[i]);
+  g.pairs = inB[0] ? 1 : 0;  // physical bit 0 is then T's and B's lowest: j bit 0
+  for (uint32_t p = 0; p < 128; ++p) split(2 * p, &g.psrc_lo[p], &g.pdst_lo[p]);
+  for (uint32_t i = 0; i < 32; ++i) split(i << 8, &g.psrc_hi[i], &g.pdst_hi[i]);
   std::memcpy(out, &g, sizeof(g));
   return true;
 }
 
-cudaError_t launch_dense6_tc_gather(void* psi, int n, const void* d_weights, const void* d_tabs, unsigned* err,
-                                    uint64_t limit_ns, cudaStream_t s) {
+cudaError_t launch_dense6_tc_gather(void* psi, int n, const void* d_weights, const void* d_tabs, bool pairs,
+                                    unsigned* err, uint64_t limit_ns, cudaStream_t s) {
   if (n < 13) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(dense6_tc_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kSmemPipe);
+  auto kern = pairs ? dense6_tc_gather_kernel<true> : dense6_tc_gather_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemPipe);
   if (e != cudaSuccess) return e;
   const uint64_t tiles = 1ull << (n - 13);
   uint64_t grid = (uint64_t)device_sm_count();
   if (grid > tiles) grid = tiles;
-  dense6_tc_gather_kernel<<<(unsigned)grid, 128, kSmemPipe, s>>>(reinterpret_cast<float2*>(psi), tiles,
-                                                                 reinterpret_cast<const uint4*>(d_weights),
-                                                                 reinterpret_cast<const GatherTabs*>(d_tabs), err,
-                                                                 limit_ns);
+  kern<<<(unsigned)grid, 128, kSmemPipe, s>>>(reinterpret_cast<float2*>(psi), tiles,
+                                              reinterpret_cast<const uint4*>(d_weights),
+                                              reinterpret_cast<const GatherTabs*>(d_tabs), err, limit_ns);
   return cudaGetLastError();
 }
 

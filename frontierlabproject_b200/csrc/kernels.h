@@ -49,11 +49,12 @@ void dense6_prepare_weights(const std::complex<double>* U, uint8_t* out);
 cudaError_t launch_dense6_tc(void* psi, int n, const void* d_weights, unsigned* err, uint64_t limit_ns,
                              cudaStream_t s);
 // the same on six arbitrary physical bits B (ascending): tables of dense6_gather_bytes() bytes
-// from dense6_gather_tables (false: fewer than 13 qubits), device copy d_tabs
+// from dense6_gather_tables (false: fewer than 13 qubits), device copy d_tabs; pairs: physical
+// bit 0 is in B (B[0] == 0), so the copies move 16-byte amplitude pairs
 size_t dense6_gather_bytes();
 bool dense6_gather_tables(int n, const int* B, uint8_t* out);
-cudaError_t launch_dense6_tc_gather(void* psi, int n, const void* d_weights, const void* d_tabs, unsigned* err,
-                                    uint64_t limit_ns, cudaStream_t s);
+cudaError_t launch_dense6_tc_gather(void* psi, int n, const void* d_weights, const void* d_tabs, bool pairs,
+                                    unsigned* err, uint64_t limit_ns, cudaStream_t s);
 
 // measurement sampling (kern_sample.cu): `shots` indices drawn from |psi|^2, ascending, into
 // out (device); scratch: sample_scratch_bytes(n, shots) bytes of device memory

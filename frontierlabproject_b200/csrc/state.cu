@@ -793,8 +793,8 @@ int qs_apply_dense(qs_state* s, int k, const int* qubits, const double* U) {
     if (low6)
       CK(launch_dense6_tc(s->psi, s->n, s->d_dense, s->d_ctl + 2, s->wait_limit_ns, s->stream));
     else
-      CK(launch_dense6_tc_gather(s->psi, s->n, s->d_dense, (const uint8_t*)s->d_dense + wbytes, s->d_ctl + 2,
-                                 s->wait_limit_ns, s->stream));
+      CK(launch_dense6_tc_gather(s->psi, s->n, s->d_dense, (const uint8_t*)s->d_dense + wbytes, b6[0] == 0,
+                                 s->d_ctl + 2, s->wait_limit_ns, s->stream));
     s->st.launches += 1;
     s->st.gate_sweeps += 1;
   });
