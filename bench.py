@@ -589,6 +589,11 @@ def main():
 
     from frontierlabproject_b200 import build as B
     B.build()
+    # cold starts are measured as cold: kernels compiled in this run go to an empty private cache
+    # (an explicit QSIM_JIT_CACHE is respected)
+    if "QSIM_JIT_CACHE" not in os.environ:
+        import tempfile
+        os.environ["QSIM_JIT_CACHE"] = tempfile.mkdtemp(prefix="qsim_jit_")
     from frontierlabproject_b200.backend import run_custom_backend
     from frontierlabproject_b200.qgpusim_cuda import StatevectorF32
     from frontierlabproject_b200.replicas import max_over_ranks, whole_job_rate

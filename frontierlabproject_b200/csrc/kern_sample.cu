@@ -1,7 +1,8 @@
 // Measurement sampling: `shots` basis indices drawn from |psi|^2 (multinomial), on the device.
 //
 //   1. block sums of |psi(x)|^2 over blocks of kSampleBlock amplitudes (FP64);
-//   2. exclusive prefix of the block sums (one-block scan kernel, FP64);
+//   2. exclusive prefix of the block sums (FP64: tiles of 4096 scanned per block, the tile totals
+//      scanned, then added back);
 //   3. sorted uniforms: u_(k) = C_k / C_{shots+1}, k = 1..shots, with C the prefix sums of
 //      shots + 1 i.i.d. Exp(1) draws (the order statistics of `shots` uniforms), scaled by
 //      the total probability;
@@ -42,7 +43,69 @@ __global__ void block_prob_kernel(const C* __restrict__ psi, uint64_t dim, doubl
   }
 }
 
-// In-place exclusive prefix of v[0..n) with one block of 1024 threads; v[n] = total.
+constexpr int kScanThreads = 256, kScanItems = 16, kScanTile = kScanThreads * kScanItems;  // 4096 per tile
+
+// Exclusive prefix of each kScanTile-element tile of v[0..n) in place (coalesced through shared
+// memory: each thread scans 16 consecutive elements, the block scans the thread totals with warp
+// shuffles); the tile's total goes to sums[tile].
+__global__ void __launch_bounds__(kScanThreads) tile_scan_kernel(double* __restrict__ v, uint64_t n,
+                                                                 double* __restrict__ sums) {
+  __shared__ double sh[kScanTile];
+  __shared__ double wsum[kScanThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint64_t i = base + t + j * kScanThreads;
+    sh[t + j * kScanThreads] = i < n ? v[i] : 0.0;
+  }
+  __syncthreads();
+  double loc[kScanItems];
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    loc[j] = s;
+    s += sh[t * kScanItems + j];
+  }
+  double incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const double w = lane < kScanThreads / 32 ? wsum[lane] : 0.0;
+    double wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kScanThreads / 32) wsum[lane] = wi - w;  // exclusive over warps
+  }
+  __syncthreads();
+  const double off = wsum[warp] + (incl - s);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) sh[t * kScanItems + j] = loc[j] + off;
+  if (t == kScanThreads - 1) sums[blockIdx.x] = off + s;
+  __syncthreads();
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint64_t i = base + t + j * kScanThreads;
+    if (i < n) v[i] = sh[t + j * kScanThreads];
+  }
+}
+
+// v[i] += pre[i / kScanTile] for i < n, and v[n] = pre[ntiles] (the total)
+__global__ void add_tile_offsets_kernel(double* __restrict__ v, uint64_t n, const double* __restrict__ pre,
+                                        uint64_t ntiles) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    v[i] += pre[i / kScanTile];
+  if (blockIdx.x == 0 && threadIdx.x == 0) v[n] = pre[ntiles];
+}
+
+// In-place exclusive prefix of v[0..n) with one block of 1024 threads; v[n] = total (for the
+// tile totals, a few thousand entries).
 __global__ void __launch_bounds__(1024) scan_kernel(double* __restrict__ v, uint64_t n) {
   __shared__ double part[1024];
   const uint64_t per = (n + 1023) / 1024;
@@ -139,11 +202,22 @@ __global__ void assign_kernel(const C* __restrict__ psi, uint64_t dim, const dou
   }
 }
 
+uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+// exclusive prefix of v[0..n) in place, v[n] = total; sums: scan_tiles(n) + 1 doubles
+void device_scan(double* v, uint64_t n, double* sums, cudaStream_t s) {
+  const uint64_t nt = scan_tiles(n);
+  tile_scan_kernel<<<(unsigned)nt, kScanThreads, 0, s>>>(v, n, sums);
+  scan_kernel<<<1, 1024, 0, s>>>(sums, nt);
+  const uint64_t g = (n + 255) / 256;
+  add_tile_offsets_kernel<<<(unsigned)(g < 4096 ? (g ? g : 1) : 4096), 256, 0, s>>>(v, n, sums, nt);
+}
+
 }  // namespace
 
 size_t sample_scratch_bytes(int n, uint64_t shots) {
   const uint64_t nb = ((1ull << n) + kSampleBlock - 1) / kSampleBlock;
-  return (nb + 1 + shots + 2) * sizeof(double);
+  return (nb + 1 + shots + 2 + scan_tiles(nb) + 1 + scan_tiles(shots + 1) + 1) * sizeof(double);
 }
 
 cudaError_t launch_sample(int dtype, const void* psi, int n, uint64_t shots, uint64_t seed, void* scratch,
@@ -152,14 +226,16 @@ cudaError_t launch_sample(int dtype, const void* psi, int n, uint64_t shots, uin
   const uint64_t nb = (dim + kSampleBlock - 1) / kSampleBlock;
   double* bsum = reinterpret_cast<double*>(scratch);   // nb + 1
   double* e = bsum + nb + 1;                           // shots + 2
+  double* sums_b = e + shots + 2;                      // scan_tiles(nb) + 1
+  double* sums_e = sums_b + scan_tiles(nb) + 1;        // scan_tiles(shots + 1) + 1
   if (dtype == 0) block_prob_kernel<float2><<<(unsigned)nb, 256, 0, s>>>((const float2*)psi, dim, bsum);
   else block_prob_kernel<double2><<<(unsigned)nb, 256, 0, s>>>((const double2*)psi, dim, bsum);
-  scan_kernel<<<1, 1024, 0, s>>>(bsum, nb);
+  device_scan(bsum, nb, sums_b, s);
   // shots + 1 draws into e[0..shots]; the exclusive scan leaves e[k+1] = sum of the first k+1
   // draws and e[shots+1] = the total
   const uint64_t g = (shots + 1 + 255) / 256;
   exp_draw_kernel<<<(unsigned)(g < 4096 ? g : 4096), 256, 0, s>>>(e, shots + 1, seed);
-  scan_kernel<<<1, 1024, 0, s>>>(e, shots + 1);
+  device_scan(e, shots + 1, sums_e, s);
   const unsigned warps_per_block = 8;
   uint64_t grid = (nb + warps_per_block - 1) / warps_per_block;
   if (grid > 65535) grid = 65535;
