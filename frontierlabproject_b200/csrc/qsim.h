@@ -31,7 +31,7 @@ namespace qsb {
 
 constexpr int kMaxQubits = 40;
 constexpr int kMaxM = 16;          // local bits per pass (group of 2^m amplitudes)
-constexpr int kMaxR = 5;           // register bits per thread
+constexpr int kMaxR = 6;           // register bits per thread (the generic kernels use 5 / 4)
 constexpr int kFixed = 64;         // operand >= kFixed: physical bit (operand - kFixed), value fixed per thread
 // dynamic shared-memory limit requested for the pass kernels (two 64 KiB group buffers);
 // static tables take about 30 KiB more, within the 227 KiB per block

@@ -837,7 +837,7 @@ int qs_set_config(qs_state* s, const qs_config* c) {
     if (c->m < reg_bits(s->dtype) + 1 || c->m > mmax) throw InvalidArg{"config: m out of range"};
     if (c->k < 1 || c->k > c->m) throw InvalidArg{"config: k out of range"};
     if (c->hill_iters < 0) throw InvalidArg{"config: hill_iters must be >= 0"};
-    if (c->jit_lr < 3 || c->jit_lr > 5 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
+    if (c->jit_lr < 3 || c->jit_lr > 6 || c->m - c->jit_lr > 9) throw InvalidArg{"config: jit_lr out of range"};
     if (c->jit_blocks < 1 || c->jit_blocks > 4) throw InvalidArg{"config: jit_blocks must be 1, 2, 3 or 4"};
     if (c->jit_packed < 0 || c->jit_packed > 1) throw InvalidArg{"config: jit_packed must be 0 or 1"};
     if (c->jit_async < 0 || c->jit_async > 1) throw InvalidArg{"config: jit_async must be 0 or 1"};
@@ -1037,7 +1037,7 @@ int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs
     for (auto& o : q) c.push_back(classify(o));
     PlanConfig pc = cfg_from(dtype, num_qubits, cfg);
     // complex64 with an explicit register-bit count: plan as the specialised kernels would
-    if (dtype == 0 && cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) pc.r = cfg->jit_lr;
+    if (dtype == 0 && cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 6) pc.r = cfg->jit_lr;
     auto passes = plan_passes(c, num_qubits, pc);
     int ph = 0;
     for (auto& p : passes) ph += (int)p.phases.size();
@@ -1052,8 +1052,11 @@ int qs_plan_emulate(int num_qubits, int dtype, const qs_op* ops, int nops, const
     auto q = convert_ops(nullptr, ops, nops, num_qubits, dtype, false);
     std::vector<COp> c;
     for (auto& o : q) c.push_back(classify(o));
-    auto passes = plan_passes(c, num_qubits, cfg_from(dtype, num_qubits, cfg));
-    Program prog = build_program(q, passes, num_qubits, dtype, 0);
+    PlanConfig pc = cfg_from(dtype, num_qubits, cfg);
+    // complex64 with an explicit register-bit count: the program the specialised kernels run
+    if (dtype == 0 && cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 6) pc.r = cfg->jit_lr;
+    auto passes = plan_passes(c, num_qubits, pc);
+    Program prog = build_program(q, passes, num_qubits, dtype, pc.r);
     emulate_program(prog.bytes.data(), psi, num_qubits, dtype);
   });
 }
@@ -1066,7 +1069,7 @@ int qs_jit_check(int num_qubits, const qs_op* ops, int nops, const qs_config* cf
     std::vector<COp> c;
     for (auto& o : q) c.push_back(classify(o));
     PlanConfig pc = cfg_from(0, num_qubits, cfg);
-    pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 5) ? cfg->jit_lr : 5;
+    pc.r = (cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 6) ? cfg->jit_lr : 5;
     pc.pair_bit = cfg && cfg->jit_packed == 1;
     auto passes = plan_passes(c, num_qubits, pc);
     Program prog = build_program(q, passes, num_qubits, 0, pc.r);

@@ -62,7 +62,8 @@ typedef struct {
   int grid_mult;  /* resident blocks per SM used by the pass kernel (0 = occupancy) */
   int jit;        /* plan-time specialised kernels in graphed mode: 0 auto (complex64,
                      >= 20 qubits), 1 always (complex64), -1 never */
-  int jit_lr;     /* register bits per thread of the specialised kernels (3..5) */
+  int jit_lr;     /* register bits per thread of the specialised kernels (3..6; 6: 64 amplitudes
+                     per thread, 2^(m-6) threads per group) */
   int jit_blocks; /* specialised kernels: 1 double-buffered block per SM, 2 single-buffered
                      blocks per SM, 3 one block of two teams over three buffers */
   int jit_packed; /* specialised kernels: FP32x2 arithmetic on two amplitudes (1) or scalar (0) */

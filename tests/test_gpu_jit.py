@@ -33,10 +33,10 @@ def test_jit_source_compiles_for_sm100a(native_lib):
             assert line.strip().startswith("0 bytes stack frame") or " 0 bytes spill stores" in line, line
 
 
-def _run_jit(qc, nl, blocks=2, packed=0, **kw):
+def _run_jit(qc, nl, blocks=2, packed=0, lr=5, **kw):
     _, plan = tile_circuit(qc, nl)
     sv = StatevectorF32(qc.num_qubits)
-    sv.set_config(jit=1, jit_blocks=blocks, jit_packed=packed)
+    sv.set_config(jit=1, jit_blocks=blocks, jit_packed=packed, jit_lr=lr)
     psi, met = run_custom_backend(qc, plan, "statevector", use_float32=True, tile_mode="graphed", sv=sv, **kw)
     return psi, met, plan, sv
 
@@ -209,3 +209,16 @@ def test_jit_async_generic_stand_in_then_specialised():
     st = sv.stats()
     assert st["jit_modules"] >= 1 and st["jit_pending_flushes"] == 0
     assert O.infidelity(ref, psi2) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("blocks", [1, 2, 3])
+@pytest.mark.parametrize("n", [14, 20])
+def test_jit_six_register_bits(n, blocks):
+    # 64 amplitudes per thread, 2^(m-6) threads per group: mixed gates and the bit-flip frame
+    for qc in (_mixed(n, n + 3), _flip_frame_circuit(n, 4)):
+        psi, _, _, sv = _run_jit(qc, n - 2, blocks, 0, 6, logical_order=True)
+        assert sv.get_config()["jit_lr"] == 6
+        ref = O.simulate(qc)
+        assert O.infidelity(ref, psi) <= 1e-5
+        assert np.max(np.abs(psi - ref)) <= 1e-5

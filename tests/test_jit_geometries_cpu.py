@@ -28,15 +28,22 @@ def _jit_check(qc, blocks, packed, lr=5):
 
 # 1 double-buffered block per SM, 2 single-buffered blocks (last phase stored from registers),
 # 3 two teams over three buffers, 4 two double-buffered blocks; packed = FP32x2 arithmetic
-@pytest.mark.parametrize("blocks,packed", [(1, 0), (2, 0), (3, 0), (4, 0), (2, 1), (3, 1)])
-def test_kernel_geometries_compile(native_lib, blocks, packed):
-    rc, sweeps, text = _jit_check(_mixed(15, 3), blocks, packed)
+@pytest.mark.parametrize("blocks,packed,lr", [(1, 0, 5), (2, 0, 5), (3, 0, 5), (4, 0, 5), (2, 1, 5), (3, 1, 5),
+                                              (2, 0, 6), (1, 0, 6), (3, 0, 6)])
+def test_kernel_geometries_compile(native_lib, blocks, packed, lr):
+    rc, sweeps, text = _jit_check(_mixed(15, 3), blocks, packed, lr)
     err = native_lib.qs_last_error()
     if rc != 0 and b"NVRTC" in err and b"not found" in err:
         pytest.skip("NVRTC unavailable")
     assert rc == 0, err.decode()
     assert sweeps >= 1
     assert "registers" in text
+    if not packed:  # interleaved registers: the amplitudes stay in registers (the packed option spills)
+        for line in text.splitlines():
+            if "spill stores" in line:
+                spilled = int(line.split("bytes spill stores")[0].split(",")[-1].strip())
+                # 6 register bits: 64 amplitudes against 255 registers leave a few bytes in some kernels
+                assert spilled <= (64 if lr == 6 else 0), line
 
 
 def _plan(qc, hill):
@@ -66,3 +73,16 @@ def test_full_search_plan_emulates_to_oracle(native_lib, seed):
     N.call("qs_plan_emulate", n, 1, b.ptr, len(b), ctypes.byref(cfg), psi.ctypes.data)
     ref = O.simulate(qc)
     assert np.max(np.abs(psi - ref)) <= 1e-12
+
+
+@pytest.mark.parametrize("lr", [4, 5, 6])
+def test_register_bit_counts_emulate_to_oracle(native_lib, lr):
+    # the program planned for 4, 5 or 6 register bits per thread (the specialised kernels' plan)
+    qc = _mixed(15, 2)
+    n = qc.num_qubits
+    b = _OpBatch(ops_of(qc), 0)
+    psi = np.zeros(1 << n, dtype=np.complex64)
+    psi[0] = 1
+    cfg = N.QsConfig(13, 3, 16, 0, 1, lr, 2, 0)
+    N.call("qs_plan_emulate", n, 0, b.ptr, len(b), ctypes.byref(cfg), psi.ctypes.data)
+    assert O.infidelity(O.simulate(qc), psi) <= 1e-6
