@@ -152,6 +152,10 @@ __device__ __forceinline__ void named_barrier(unsigned id, unsigned nthreads) {
 }
 
 constexpr int kPassThreads = 256;
+// load/store item rows per thread and group: 2^(r - 1) for complex64 (16-byte pairs), 2^r for
+// complex128; r <= 6 (complex64) and r <= 4 (complex128) keep it within 32
+constexpr int kMaxItems = 32;
+static_assert(kMaxItems >= (1 << (kMaxR - 1)), "item tables too small for the register bits");
 
 // Issue the asynchronous load of the group with physical base `gbase` into the shared buffer
 // `buf` (16-byte copies, swizzled destinations).  Items: c64 -> two amplitudes (local bit 0
@@ -166,8 +170,8 @@ __device__ __forceinline__ void prefetch_group(typename V2<Real>::T* buf, const 
   if ((int)t >= T) return;
   const uint32_t lt = (uint32_t)t << kItemBits;
   const uint64_t base = gbase | tbase;
-#pragma unroll(kUnroll ? 16 : 1)
-  for (int v = 0; v < 16; ++v) {
+#pragma unroll(kUnroll ? kMaxItems : 1)
+  for (int v = 0; v < kMaxItems; ++v) {
     if (v >= V) break;
     const uint32_t l = lt | (((uint32_t)v * (uint32_t)T) << kItemBits);
     cp_async16(buf + swz<Real>(l), psi + (base | pv[v]));
@@ -275,10 +279,10 @@ struct PassShared {
   uint64_t gtab[5 * 128];        // group index -> physical base (5 levels x 7 bits)
   uint64_t pt[kPhaseTab * 48];   // per phase: physical thread base, t bits 0-3 | 4-8
   uint64_t base[512];            // per thread: physical offset of its first item
-  uint64_t pv[16];               // physical offset of load/store item row v
+  uint64_t pv[kMaxItems];        // physical offset of load/store item row v
   uint32_t lt[kPhaseTab * 48];   // per phase: local thread base
   uint32_t stt[512];             // per thread: store-permutation source of its first item
-  uint32_t sv[16];               // store-permutation source local offset of row v
+  uint32_t sv[kMaxItems];        // store-permutation source local offset of row v
   PassDesc pd;
 };
 
@@ -293,7 +297,7 @@ __device__ __forceinline__ void pass_setup(PassShared& sh, const uint8_t* __rest
   const PassDesc& pd = sh.pd;
   const int m = pd.m;
   const int T = 1 << (m - pd.r);                    // active threads of this pass (per team)
-  const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (16)
+  const int V = 1 << (m - kItemBits) >> (m - pd.r);  // items per thread (<= kMaxItems)
   const int nt = m - pd.r;                           // thread-index bits
   for (int v = t; v < V; v += nthr) {
     const uint32_t lv = ((uint32_t)v * (uint32_t)T) << kItemBits;
@@ -452,7 +456,7 @@ __device__ __forceinline__ void group_store(const PassShared& sh, typename V2<Re
   const uint32_t stt = sh.stt[t];
   if constexpr (kC64) {
 #pragma unroll
-    for (int v = 0; v < 16; ++v) {
+    for (int v = 0; v < kMaxItems; ++v) {
       if (v >= V) break;
       float4 val;
       if (pd.store_perm) {
@@ -469,7 +473,7 @@ __device__ __forceinline__ void group_store(const PassShared& sh, typename V2<Re
     }
   } else {
 #pragma unroll
-    for (int v = 0; v < 16; ++v) {
+    for (int v = 0; v < kMaxItems; ++v) {
       if (v >= V) break;
       const uint32_t l = lt | ((uint32_t)v * (uint32_t)T);
       const uint32_t src = pd.store_perm ? (stt | sh.sv[v]) : l;

@@ -213,7 +213,7 @@ def test_jit_async_generic_stand_in_then_specialised():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("blocks", [1, 2, 3])
-@pytest.mark.parametrize("n", [14, 20])
+@pytest.mark.parametrize("n", [16, 20])
 def test_jit_six_register_bits(n, blocks):
     # 64 amplitudes per thread, 2^(m-6) threads per group: mixed gates and the bit-flip frame
     for qc in (_mixed(n, n + 3), _flip_frame_circuit(n, 4)):
