@@ -85,6 +85,13 @@ _SIGS = {
     "qs_inner_product": [c_void_p, c_void_p, POINTER(c_double), POINTER(c_double)],
     "qs_expect_zz_x": [c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_double)],
     "qs_adjoint_sweep": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int],
+    "qs_grad_create": [c_int, c_void_p, c_int, c_int, c_void_p, POINTER(c_void_p)],
+    "qs_grad_run": [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p],
+    "qs_grad_info": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    "qs_grad_stats": [c_void_p, c_void_p],
+    "qs_grad_destroy": [c_void_p],
+    "qs_grad_emulate": [c_int, c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p],
+    "qs_grad_jit_check": [c_int, c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
     "qs_apply_1q_gate": [c_void_p, c_int, c_void_p, c_int, c_int, c_void_p],
     "qs_apply_2q_gate": [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p],
     "qs_permute_scatter": [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p],
@@ -109,6 +116,7 @@ _SIGS = {
     "qs_batch_info": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
     "qs_batch_destroy": [c_void_p],
     "qs_batch_emulate": [c_void_p, c_int, c_void_p, c_void_p, c_void_p],
+    "qs_batch_describe": [c_void_p, c_int, c_void_p, c_void_p],
 }
 
 _lib = None

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
 
@@ -30,6 +31,53 @@ ADJ_OP = np.dtype({"names": ["kind", "q0", "q1", "gen", "grad_index", "pad", "U"
                    "formats": ["<i4", "<i4", "<i4", "<i4", "<i4", "<i4", "<u8"],
                    "offsets": [0, 4, 8, 12, 16, 20, 24], "itemsize": 32})
 GEN = {"rx": 1, "ry": 2, "rz": 3}
+
+
+class AdjOps:
+    """The ``qs_adj_op`` table of a ParamCircuit (complex128 matrices in one buffer).  ``update``
+    rewrites the rotations' matrices for new parameters in place (numpy over all gates of a
+    generator at once); fixed gates are computed once.  The table points into this object's
+    buffer: keep the object alive while the table is in use."""
+
+    def __init__(self, pc: "ParamCircuit"):
+        G = len(pc.gates)
+        self.ops = np.zeros(G, dtype=ADJ_OP)
+        sizes = np.array([4 if len(g.qubits) == 1 else 16 for g in pc.gates], dtype=np.int64)
+        off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        self.buf = np.zeros(int(off[-1]), dtype=np.complex128)
+        base = self.buf.ctypes.data
+        rot = {1: ([], []), 2: ([], []), 3: ([], [])}
+        for i, g in enumerate(pc.gates):
+            o = self.ops[i]
+            o["kind"] = len(g.qubits)
+            o["q0"] = g.qubits[0]
+            o["q1"] = g.qubits[1] if len(g.qubits) > 1 else -1
+            o["U"] = base + 16 * int(off[i])
+            if g.param is not None:
+                if g.name not in GEN:
+                    raise ValueError(f"parameterised gate {g.name!r} is not a single-qubit rotation")
+                o["gen"] = GEN[g.name]
+                o["grad_index"] = g.param
+                rot[GEN[g.name]][0].append(int(off[i]))
+                rot[GEN[g.name]][1].append(g.param)
+            else:
+                self.buf[off[i]:off[i + 1]] = np.asarray(gate_matrix(g.name, g.fixed), dtype=np.complex128).reshape(-1)
+        self.rot = {k: (np.array(v[0], dtype=np.int64), np.array(v[1], dtype=np.int64)) for k, v in rot.items() if v[0]}
+
+    def update(self, theta) -> np.ndarray:
+        th = np.asarray(theta, dtype=np.float64)
+        for gen, (offs, slots) in self.rot.items():
+            h = 0.5 * th[slots]
+            c, s = np.cos(h), np.sin(h)
+            if gen == 1:
+                M = np.stack([c, -1j * s, -1j * s, c], axis=1)
+            elif gen == 2:
+                M = np.stack([c, -s, s, c], axis=1).astype(np.complex128)
+            else:
+                z = np.zeros_like(c)
+                M = np.stack([np.exp(-1j * h), z, z, np.exp(1j * h)], axis=1)
+            self.buf[offs[:, None] + np.arange(4)] = M
+        return self.ops
 
 
 @dataclass
@@ -83,25 +131,48 @@ class AdjointEngine:
     """Energy and gradient of ``ParamCircuit`` expectations on one GPU."""
 
     def __init__(self, num_qubits: int, f32: bool = True, mode: str = "graphed", method: str = "auto"):
-        """method: "fused" (complex64: the whole gradient in one persistent launch of the
-        batched kernel, planned passes over psi and lam), "per_gate" (one reverse kernel per
-        gate over the two states), "auto" (fused for complex64 with 2..26 qubits)."""
+        """method: "jit" (complex64, 10..33 qubits: the forward tile and ONE reverse program over
+        the stacked state psi (+) H psi, both with the plan-time specialised kernels),
+        "fused" (complex64: the whole gradient in one persistent launch of the batched kernel,
+        planned passes over psi and lam), "per_gate" (one reverse kernel per gate over the two
+        states), "auto" (jit for complex64 with 14..33 qubits when NVRTC is available, fused
+        for 2..13, per_gate otherwise)."""
         cls = StatevectorF32 if f32 else Statevector
         self.n = num_qubits
         self.f32 = f32
         self.mode = mode
-        if method not in ("auto", "fused", "per_gate"):
+        if method not in ("auto", "jit", "fused", "per_gate"):
             raise ValueError(f"unknown method: {method}")
-        if method == "fused" and not f32:
-            raise ValueError("the fused gradient runs complex64 states")
-        self.method = "fused" if (method == "auto" and f32 and 2 <= num_qubits <= 26) else \
-            ("per_gate" if method == "auto" else method)
-        self.psi = cls(num_qubits)
-        self.lam = cls(num_qubits)
+        if method in ("fused", "jit") and not f32:
+            raise ValueError(f"the {method} gradient runs complex64 states")
+        if method == "jit" and not 10 <= num_qubits <= 33:
+            raise ValueError("the jit gradient needs 10..33 qubits")
+        if method == "auto":
+            if f32 and 14 <= num_qubits <= 33 and _jit_available():
+                method = "jit"
+            elif f32 and 2 <= num_qubits <= 26:
+                method = "fused"
+            else:
+                method = "per_gate"
+        self.method = method
+        self.psi = None if method == "jit" else cls(num_qubits)
+        self.lam = None if method == "jit" else cls(num_qubits)
         self._np_dtype = np.complex64 if f32 else np.complex128
         self._fused = None      # (structure key, BatchedAdjoint)
+        self._grad = None       # (structure key, qs_grad handle, AdjOps)
+
+    def __del__(self):
+        g = getattr(self, "_grad", None)
+        if g is not None:
+            try:
+                N.lib().qs_grad_destroy(g[1])
+            except Exception:  # interpreter shutdown: the library may already be unloaded
+                pass
+            self._grad = None
 
     def set_config(self, **kw) -> None:
+        if self.method == "jit":
+            raise ValueError("the jit gradient plans with its own configuration")
         self.psi.set_config(**kw)
         self.lam.set_config(**kw)
 
@@ -122,6 +193,8 @@ class AdjointEngine:
         return mats
 
     def energy(self, pc: ParamCircuit, theta, a, b) -> float:
+        if self.method == "jit":
+            return self._jit_energy_and_grad(pc, theta, a, b, grad=False)[0]
         self._forward(pc, theta)
         return self._expect(a, b)
 
@@ -135,9 +208,48 @@ class AdjointEngine:
         return e.value
 
     def energy_and_grad(self, pc: ParamCircuit, theta, a, b) -> Tuple[float, np.ndarray]:
+        if self.method == "jit":
+            return self._jit_energy_and_grad(pc, theta, a, b)
         if self.method == "fused":
             return self._fused_energy_and_grad(pc, theta, a, b)
         return self._per_gate_energy_and_grad(pc, theta, a, b)
+
+    def _jit_energy_and_grad(self, pc: ParamCircuit, theta, a, b, grad: bool = True) -> Tuple[float, np.ndarray]:
+        if pc.num_qubits != self.n:
+            raise ValueError("circuit size differs from the engine's")
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if a.size != self.n or b.size != self.n:
+            raise ValueError("observable coefficients must have num_qubits entries")
+        key = (tuple((g.name, g.qubits, g.param, g.fixed) for g in pc.gates), pc.num_params)
+        if self._grad is None or self._grad[0] != key:
+            if self._grad is not None:
+                N.lib().qs_grad_destroy(self._grad[1])
+                self._grad = None
+            tab = AdjOps(pc)
+            ops = tab.update(theta)
+            h = ctypes.c_void_p()
+            N.call("qs_grad_create", self.n, ops.ctypes.data, len(ops), pc.num_params, None, ctypes.byref(h))
+            self._grad = (key, h, tab)
+        h, tab = self._grad[1], self._grad[2]
+        ops = tab.update(theta)
+        E = ctypes.c_double()
+        G = np.zeros(pc.num_params, dtype=np.float64)
+        N.call("qs_grad_run", h, ops.ctypes.data, len(ops), a.ctypes.data, b.ctypes.data, ctypes.byref(E),
+               G.ctypes.data if grad else None)
+        return float(E.value), G
+
+    def info(self) -> dict:
+        """jit method: sweeps of the last forward run and of the reverse program, register phases
+        of the reverse program, gradient terms, and the handle's execution counters."""
+        if self._grad is None:
+            return {}
+        fs, rs, ph, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.call("qs_grad_info", self._grad[1], ctypes.byref(fs), ctypes.byref(rs), ctypes.byref(ph), ctypes.byref(nt))
+        st = N.QsStats()
+        N.call("qs_grad_stats", self._grad[1], ctypes.byref(st))
+        return {"forward_sweeps": fs.value, "reverse_sweeps": rs.value, "reverse_phases": ph.value,
+                "terms": nt.value, **st.as_dict()}
 
     def _fused_energy_and_grad(self, pc: ParamCircuit, theta, a, b) -> Tuple[float, np.ndarray]:
         from .batch import BatchedAdjoint, BatchShape, Instance
@@ -183,6 +295,31 @@ class AdjointEngine:
             tm[k] -= math.pi / 2
             out[j] = 0.5 * (self.energy(pc, tp, a, b) - self.energy(pc, tm, a, b))
         return out
+
+
+def _jit_available() -> bool:
+    """NVRTC (the specialised kernels' compiler) can be loaded."""
+    import ctypes.util
+    for name in ("libnvrtc.so.12", "libnvrtc.so"):
+        try:
+            ctypes.CDLL(name)
+            return True
+        except OSError:
+            continue
+    return os.path.exists("/usr/local/cuda/lib64/libnvrtc.so.12")
+
+
+def grad_emulate(pc: ParamCircuit, theta, psi: np.ndarray, lam: np.ndarray) -> np.ndarray:
+    """Host interpretation of the jit method's reverse program (CPU tests): gradients from the
+    final state psi = U|0> and lam = H psi (complex64)."""
+    tab = AdjOps(pc)
+    ops = tab.update(theta)
+    psi = np.ascontiguousarray(psi, dtype=np.complex64)
+    lam = np.ascontiguousarray(lam, dtype=np.complex64)
+    G = np.zeros(pc.num_params, dtype=np.float64)
+    N.call("qs_grad_emulate", pc.num_qubits, ops.ctypes.data, len(ops), pc.num_params, None, psi.ctypes.data,
+           lam.ctypes.data, G.ctypes.data)
+    return G
 
 
 def _torch_function():

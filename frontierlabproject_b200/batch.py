@@ -121,6 +121,17 @@ def emulate(insts: Sequence[Instance], shape: BatchShape = BatchShape()) -> Tupl
     return E, P.split(G)
 
 
+def describe(insts: Sequence[Instance], shape: BatchShape = BatchShape()) -> List[Dict[str, int]]:
+    """Host-side plan of the batch, per instance: passes, passes run in register phases,
+    register phases, gates and work items (no device work)."""
+    P = _Packed(insts)
+    S = np.zeros(5 * len(insts), dtype=np.int32)
+    cfg = shape.c()
+    N.call("qs_batch_describe", ctypes.cast(P.arr, ctypes.c_void_p), len(insts), ctypes.byref(cfg), S.ctypes.data)
+    keys = ("passes", "register_passes", "phases", "gates", "items")
+    return [dict(zip(keys, map(int, S[5 * i:5 * i + 5]))) for i in range(len(insts))]
+
+
 class BatchedAdjoint:
     """One device batch: ``run`` launches the persistent kernel, ``results`` waits and returns
     (energies, per-instance gradients); ``update`` sets new parameters / observables."""

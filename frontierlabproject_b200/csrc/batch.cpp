@@ -668,6 +668,31 @@ int qs_batch_destroy(qs_batch* b) {
   return bguard([&] { delete b; });
 }
 
+int qs_batch_describe(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, int* stats) {
+  return bguard([&] {
+    if (!stats) bad("batch_describe: null stats");
+    const Cfg c = cfg_of(cfg);
+    auto in = read_instances(insts, ninst);
+    Encoded e = encode_batch(in, c);
+    BatchHeader h;
+    std::memcpy(&h, e.bytes.data(), sizeof(h));
+    const BatchInst* bi = reinterpret_cast<const BatchInst*>(e.bytes.data() + h.off_inst);
+    const BatchPass* bp = reinterpret_cast<const BatchPass*>(e.bytes.data() + h.off_pass);
+    const BatchItem* it = reinterpret_cast<const BatchItem*>(e.bytes.data() + h.off_item);
+    for (int i = 0; i < ninst; ++i) {
+      int* s = stats + 5 * i;
+      s[0] = bi[i].npass;
+      s[1] = s[2] = s[3] = s[4] = 0;
+      for (int p = bi[i].pass0; p < bi[i].pass0 + bi[i].npass; ++p) {
+        s[1] += bp[p].nphase > 0;
+        s[2] += bp[p].nphase;
+        s[3] += bp[p].ngate;
+      }
+    }
+    for (int k = 0; k < h.nitem; ++k) stats[5 * it[k].inst + 4] += 1;
+  });
+}
+
 int qs_batch_emulate(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, double* energies,
                      double* grads) {
   return bguard([&] {

@@ -683,6 +683,39 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
   G.post.str("");
 }
 
+// Gradient programs: before a parameterised gate (generator gen on the instruction's operand),
+// the thread's part of Im <lam|G|psi> over its registers (register bit A holds the lam bit),
+// reduced over the warp and added to the block's term `local` (shared memory, FP64).  A
+// fixed operand only occurs for Z (a diagonal gate): its sign is the thread's bit.  Under a
+// flipped frame bit the registers of the gate's bit hold X-conjugated data: X G X = -G for
+// Y and Z.
+void gen_term(Gen& G, const GateInstr& g, int gen, int local, int A) {
+  auto& o = G.o;
+  if (A < 0 || !G.mask[A].empty()) throw std::runtime_error("jit: the lam bit is not a plain register bit");
+  const std::string AM = std::to_string(1 << A);
+  o << "{float gv=0.f;";
+  if (g.a >= kFixed) {
+    if (gen != 3) throw std::runtime_error("jit: an X or Y rotation on a fixed bit");
+    o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << AM << ")){const float2 p=a[i],l=a[i|" << AM
+      << "];gv+=l.x*p.y-l.y*p.x;}\nif(" << bitcond(g.a - kFixed) << ")gv=-gv;";
+  } else {
+    const int J = g.a;
+    if (J == A) throw std::runtime_error("jit: a gate on the lam bit");
+    const std::string JM = std::to_string(1 << J), AJ = std::to_string((1 << A) | (1 << J));
+    G.masked({J}, [&](unsigned cm) {
+      const bool flip = cm != 0 && gen != 1;
+      o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << AJ << ")){const float2 p0=a[i],p1=a[i|" << JM
+        << "],l0=a[i|" << AM << "],l1=a[i|" << AJ << "];gv" << (flip ? "-=" : "+=");
+      if (gen == 1) o << "(l0.x*p1.y-l0.y*p1.x)+(l1.x*p0.y-l1.y*p0.x);}\n";
+      else if (gen == 2) o << "(l1.x*p0.x+l1.y*p0.y)-(l0.x*p1.x+l0.y*p1.y);}\n";
+      else o << "(l0.x*p0.y-l0.y*p0.x)-(l1.x*p1.y-l1.y*p1.x);}\n";
+    });
+  }
+  o << "gv+=__shfl_xor_sync(0xffffffffu,gv,16);gv+=__shfl_xor_sync(0xffffffffu,gv,8);"
+    << "gv+=__shfl_xor_sync(0xffffffffu,gv,4);gv+=__shfl_xor_sync(0xffffffffu,gv,2);"
+    << "gv+=__shfl_xor_sync(0xffffffffu,gv,1);if((threadIdx.x&31u)==0u)atomicAdd(ga+" << local << ",(double)gv);}\n";
+}
+
 const char* kPrelude = R"(
 #include "pass_body.cuh"
 __device__ __forceinline__ float2 ldk_(const float2* p) {
@@ -717,6 +750,10 @@ uint64_t jit_key(const Program& prog, const JitConfig& cfg) {
   for (int i = 0; i < hdr->ncoef; ++i) cls[i] = (uint8_t)cls_of(cf[2 * i], cf[2 * i + 1]);
   h = fnv(h, cls.data(), cls.size());
   h = fnv(h, &cfg.blocks, sizeof(cfg.blocks));
+  if (!prog.grad_gen.empty()) {
+    h = fnv(h, prog.grad_gen.data(), prog.grad_gen.size());
+    h = fnv(h, prog.grad_term.data(), prog.grad_term.size() * sizeof(int32_t));
+  }
   const int pk = cfg.packed ? 1 : 0;
   return fnv(h, &pk, sizeof(pk));
 }
@@ -733,11 +770,27 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
   G.coef = (const float*)(b + hdr->off_coef);
   G.o << kPrelude;
   char kname[64];
+  const bool grad = !prog.grad_gen.empty();
   for (int p = pass_begin; p < pass_end; ++p) {
     const PassDesc& pd = pds[p];
     pass_coef_range(b, p, &G.kbase, &G.kcount);
+    // gradient programs: the pass's terms [t0, t0 + nt) (numbered in instruction order)
+    int t0 = 0, nt = 0;
+    if (grad) {
+      int lo = -1, hi = -1;
+      for (int h = 0; h < pd.nphase; ++h) {
+        const PhaseDesc& ph = phs[pd.phase0 + h];
+        for (int gi = 0; gi < ph.ngate; ++gi) {
+          const int t = prog.grad_term[ph.gate0 + gi];
+          if (t < 0) continue;
+          if (lo < 0) lo = t;
+          hi = t + 1;
+        }
+      }
+      if (lo >= 0) { t0 = lo; nt = hi - lo; }
+    }
     // packed registers when every phase holds local bit 0 in register bit 0
-    bool packed = cfg.packed && pd.nphase > 0 && !pd.store_perm;
+    bool packed = cfg.packed && pd.nphase > 0 && !pd.store_perm && !grad;
     for (int h = 0; h < pd.nphase && packed; ++h)
       if (phs[pd.phase0 + h].rbit[0] != 0) packed = false;
     G.packed = packed;
@@ -747,8 +800,8 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     // the pass's struct X is generated first: its splats size the parameter block
     std::ostringstream outer;
     outer.swap(G.o);
-    G.o << "struct X" << p << "{const KP" << p << "* kp;\nstatic constexpr bool kPacked=" << (packed ? "true" : "false")
-        << ";\n";
+    G.o << "struct X" << p << "{const KP" << p << "* kp;" << (grad ? "double* ga;" : "")
+        << "\nstatic constexpr bool kPacked=" << (packed ? "true" : "false") << ";\n";
     // swizzled byte offsets of each phase's register bits: immediates
     G.o << "template<typename Real,int LR>__device__ __forceinline__ void reg_offsets(const qsb::PhaseDesc*,int h,"
         << "uint32_t (&B)[LR])const{switch(h){";
@@ -813,8 +866,19 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       // Diagonal gates on fixed bits commute with every gate of the phase: their factors
       // are accumulated first, then folded into the register gate where that costs least
       // (else one multiply of every amplitude at the end of the phase).
+      // gradient programs: the register bit of the lam bit (local bit 0)
+      int A = -1;
+      for (int j = 0; j < pd.r; ++j)
+        if (ph.rbit[j] == 0) A = j;
+      auto term = [&](int gi) {
+        const int k = ph.gate0 + gi;
+        if (grad && prog.grad_gen[k]) gen_term(G, gis[k], prog.grad_gen[k], prog.grad_term[k] - t0, A);
+      };
       for (int gi = 0; gi < ph.ngate; ++gi)
-        if (fixed_diag(gis[ph.gate0 + gi])) gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+        if (fixed_diag(gis[ph.gate0 + gi])) {
+          term(gi);  // the phase's registers are untouched yet: Z of a fixed bit commutes with the phase
+          gen_gate(G, gis[ph.gate0 + gi], pd, ph);
+        }
       int absorber = -1;
       if (G.used_fa) {
         // packed kernels: only gates on register bit 0 (single-lane arithmetic) absorb; the
@@ -831,7 +895,10 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         }
       }
       for (int gi = 0; gi < ph.ngate; ++gi)
-        if (!fixed_diag(gis[ph.gate0 + gi])) gen_gate(G, gis[ph.gate0 + gi], pd, ph, gi == absorber);
+        if (!fixed_diag(gis[ph.gate0 + gi])) {
+          term(gi);
+          gen_gate(G, gis[ph.gate0 + gi], pd, ph, gi == absorber);
+        }
       if (G.used_fa && absorber < 0) {
         Ent d;
         d.cls = 7;
@@ -859,6 +926,21 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
     // with no load instruction and no register.
     const bool teams = cfg.blocks == 3;
     const int per_sm = teams ? 1 : cfg.blocks == 4 ? 2 : cfg.blocks;  // resident blocks per SM
+    const bool all_active_g = (1 << (pd.m - pd.r)) == hdr->max_threads;
+    if (grad) {
+      // the block's terms in shared memory (zeroed before the pass body's first barrier),
+      // added to the program's term array once at the end
+      if (cfg.blocks != 2 || !all_active_g || pd.nphase == 0)
+        throw std::runtime_error("jit: gradient programs run single-buffered blocks with every thread active");
+      G.o << "extern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ",2) " << kname
+          << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
+          << "double* __restrict__ gterm,const __grid_constant__ KP" << p << " kp){__shared__ double ga_["
+          << std::max(1, nt) << "];for(int j=threadIdx.x;j<" << nt << ";j+=blockDim.x)ga_[j]=0.0;const X" << p
+          << " ex{&kp,ga_};qsb::pass_body_direct<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi,"
+          << p << ");__syncthreads();for(int j=threadIdx.x;j<" << nt << ";j+=blockDim.x){const double v=ga_[j];"
+          << "if(v!=0.0)atomicAdd(gterm+" << t0 << "+j,v);}}\n";
+      continue;
+    }
     G.o << "extern \"C\" __global__ void __launch_bounds__("
         << (teams ? 2 : 1) * hdr->max_threads << "," << per_sm << ") " << kname
         << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
@@ -1083,6 +1165,7 @@ std::shared_ptr<JitKernels> jit_get(const Program& prog, const JitConfig& cfg_in
   auto k = std::make_shared<JitKernels>();
   k->key = key;
   k->blocks = cfg.blocks;
+  k->grad = !prog.grad_gen.empty();
   for (int c = 0; c < nchunk; ++c) k->disk_hits += hit[c];
   k->chunks = nchunk;
   k->cbase.resize(npass);
@@ -1161,7 +1244,7 @@ void jit_wait_all() {
 }
 
 cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
-                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream) {
+                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream, double* gterm) {
   static const float2 kNone = {0.f, 0.f};
   // the driver copies the parameter block (the pass's coefficients) at the launch call
   const float2* hc = (const float2*)host_coef;
@@ -1181,7 +1264,12 @@ cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const 
     }
     kp = block.data();
   }
-  void* args[] = {(void*)&d_prog, (void*)&psi, (void*)&err, const_cast<void*>(kp)};
+  void* args[] = {(void*)&d_prog, (void*)&psi, (void*)&err, const_cast<void*>(kp), nullptr};
+  if (k.grad) {
+    if (!gterm) return cudaErrorInvalidValue;
+    args[3] = (void*)&gterm;
+    args[4] = const_cast<void*>(kp);
+  }
   const unsigned smem = (unsigned)jit_smem_bytes(k.blocks, smem_double);
   const bool teams = k.blocks == 3;
   const int per_sm = teams ? 1 : k.blocks == 4 ? 2 : k.blocks;

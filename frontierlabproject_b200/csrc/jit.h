@@ -35,6 +35,7 @@ struct JitKernels {
                                               // (table entry * 4 + component: x, y, -x, -y)
   uint64_t key = 0;
   int blocks = 1;
+  bool grad = false;    // gradient program: the kernels take the term array (jit_launch gterm)
   double compile_seconds = 0.0;
   int chunks = 0;       // compiled modules
   int disk_hits = 0;    // of which read from the on-disk cache
@@ -68,9 +69,11 @@ void jit_wait_all();
 // host_coef = the program's coefficient table in host memory: the pass's range of it is
 // copied into the launch's parameter block.  smem_double = bytes of two group buffers
 // (Program::max_smem); threads = the program's team size; err = device error word (bounded
-// waits of the two-team kernels).
+// waits of the two-team kernels); gterm = the FP64 term array of a gradient program (its
+// kernels add their terms there; ignored otherwise).
 cudaError_t jit_launch(const JitKernels& k, int p, const uint8_t* d_prog, const void* host_coef, void* psi,
-                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream);
+                       unsigned* err, int threads, size_t smem_double, int sms, cudaStream_t stream,
+                       double* gterm = nullptr);
 
 // Dynamic shared memory of a specialised kernel: group buffers for the geometry.
 inline size_t jit_smem_bytes(int blocks, size_t smem_double) {

@@ -42,7 +42,9 @@ __device__ __forceinline__ void block_add(double v, double* acc) {
   __syncthreads();
 }
 
-template <typename C>
+// kStack (complex64): lam receives the stacked state of the gradient sweep instead,
+// lam[2x] = psi[x] and lam[2x + 1] = (H psi)[x] (one 16-byte store).
+template <typename C, bool kStack = false>
 __global__ void zz_x_kernel(const C* __restrict__ psi, C* __restrict__ lam, int n, Coef cf, double* energy) {
   const uint64_t dim = 1ull << n;
   double e = 0.0;
@@ -60,10 +62,14 @@ __global__ void zz_x_kernel(const C* __restrict__ psi, C* __restrict__ lam, int 
       re += cf.b[i] * q.x;
       im += cf.b[i] * q.y;
     }
-    C out;
-    out.x = re;
-    out.y = im;
-    lam[x] = out;
+    if constexpr (kStack) {
+      reinterpret_cast<float4*>(lam)[x] = make_float4(p.x, p.y, (float)re, (float)im);
+    } else {
+      C out;
+      out.x = re;
+      out.y = im;
+      lam[x] = out;
+    }
     e += (double)p.x * re + (double)p.y * im;
   }
   block_add(e, energy);
@@ -165,6 +171,16 @@ cudaError_t launch_zz_x(int dtype, const void* psi, void* lam, int n, const doub
   const int grid = grid_of(1ull << n, th);
   if (dtype == 0) zz_x_kernel<float2><<<grid, th, 0, s>>>((const float2*)psi, (float2*)lam, n, cf, energy);
   else zz_x_kernel<double2><<<grid, th, 0, s>>>((const double2*)psi, (double2*)lam, n, cf, energy);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zz_x_stack(const void* psi, void* phi, int n, const double* a, const double* b, double* energy,
+                              cudaStream_t s) {
+  Coef cf;
+  for (int i = 0; i < 40; ++i) { cf.a[i] = i < n ? a[i] : 0.0; cf.b[i] = i < n ? b[i] : 0.0; }
+  const int th = 256;
+  const int grid = grid_of(1ull << n, th);
+  zz_x_kernel<float2, true><<<grid, th, 0, s>>>((const float2*)psi, (float2*)phi, n, cf, energy);
   return cudaGetLastError();
 }
 

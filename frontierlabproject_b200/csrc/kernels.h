@@ -32,6 +32,10 @@ cudaError_t launch_set_basis(int dtype, void* psi, int n, uint64_t index, cudaSt
 // adjoint differentiation (kern_adjoint.cu)
 cudaError_t launch_zz_x(int dtype, const void* psi, void* lam, int n, const double* a, const double* b,
                         double* energy, cudaStream_t s);
+// Stacked state of the gradient sweep (complex64): phi[2x] = psi[x], phi[2x + 1] = (H psi)[x]
+// (2^(n+1) amplitudes), energy += <psi|H psi> (FP64).
+cudaError_t launch_zz_x_stack(const void* psi, void* phi, int n, const double* a, const double* b, double* energy,
+                              cudaStream_t s);
 cudaError_t launch_adjoint_gate1(int dtype, void* psi, void* lam, int n, int q, const std::complex<double>* Ud,
                                  int gen, double* acc, cudaStream_t s);
 cudaError_t launch_adjoint_gate2(int dtype, void* psi, void* lam, int n, int q0, int q1,

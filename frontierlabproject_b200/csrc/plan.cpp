@@ -167,7 +167,7 @@ Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& pas
   return encode_program(passes, cops, n, dtype, r);
 }
 
-void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops) {
+void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops, bool diag_absorbs) {
   cplx total(1.0, 0.0);
   int absorber = -1, absorber_cost = -1;
   // Dividing a gate by its pivot p scales the state by 1/|p| until the pass's scalar is
@@ -217,13 +217,15 @@ void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_op
     }
     // absorber: a gate whose shape survives scaling, and whose cost grows least
     const COp c0 = classify(o);
-    const bool can_absorb = o.arity == 1 || c0.kind == GK_2Q_DIAG || c0.kind == GK_2Q_DENSE;
+    bool can_absorb = o.arity == 1 || c0.kind == GK_2Q_DIAG || c0.kind == GK_2Q_DENSE;
+    if (!diag_absorbs && (c0.kind == GK_1Q_DIAG || c0.kind == GK_2Q_DIAG)) can_absorb = false;
     if (!can_absorb) continue;
     int grow = 0;
     for (int k = 0; k < d * d; ++k) grow += (o.U[k] == cplx(0, 0)) ? 0 : 4 - entry_cost(o.U[k]);
     if (absorber < 0 || grow < absorber_cost) { absorber = oi; absorber_cost = grow; }
   }
   if (total == cplx(1.0, 0.0)) return;
+  if (absorber < 0 && !diag_absorbs && std::abs(std::abs(total) - 1.0) < 1e-9) return;  // a phase
   if (absorber < 0) throw std::runtime_error("planner: no gate of the pass can absorb its scalar");
   QOp& a = ops[absorber];
   const int d = a.arity == 1 ? 2 : 4;
@@ -694,8 +696,18 @@ Program encode_program(const std::vector<PlannedPass>& passes, const std::vector
 // ---------------------------------------------------------------------------------
 // Host interpretation of a program: gate semantics by physical bit, no thread mapping.
 // ---------------------------------------------------------------------------------
+// A diagonal gate whose bits are all fixed in its phase: the specialised kernels apply it as a
+// per-thread factor, at a point of the phase of their choosing (it commutes with the phase).
+static bool fixed_diag_instr(const GateInstr& g) {
+  return (g.kind == GK_1Q_DIAG && g.a >= kFixed) || (g.kind == GK_2Q_DIAG && g.a >= kFixed && g.b >= kFixed);
+}
+
+// gen / term (optional): gradient annotations of a gradient program; psi is then the stacked
+// state (bit 0 selects lam) and terms[t] receives Im <lam|G|psi> before gate t's instruction
+// (the terms of fixed diagonal gates at the start of their phase, as the kernels take them).
 template <typename R>
-static void emulate_t(const uint8_t* prog, std::complex<R>* psi, int n) {
+static void emulate_t(const uint8_t* prog, std::complex<R>* psi, int n, const int8_t* gen = nullptr,
+                      const int32_t* term = nullptr, double* terms = nullptr) {
   using C = std::complex<R>;
   const ProgramHeader* hdr = (const ProgramHeader*)prog;
   const PassDesc* pd = (const PassDesc*)(prog + hdr->off_pass);
@@ -704,13 +716,38 @@ static void emulate_t(const uint8_t* prog, std::complex<R>* psi, int n) {
   const C* cf = (const C*)(prog + hdr->off_coef);
   const uint64_t dim = 1ull << n;
   std::vector<C> tmp;
+  // Im sum_x conj(lam(x)) (G psi)(x), G on physical bit pb (psi at even, lam at odd indices)
+  auto grad_term = [&](int pb, int g) {
+    const uint64_t mp = 1ull << pb;
+    double s = 0.0;
+    for (uint64_t i = 0; i < dim; i += 2) {
+      const std::complex<double> l(psi[i | 1].real(), psi[i | 1].imag());
+      std::complex<double> v;
+      if (g == 3) {
+        v = std::complex<double>(psi[i].real(), psi[i].imag());
+        if (i & mp) v = -v;
+      } else {
+        const std::complex<double> o(psi[i ^ mp].real(), psi[i ^ mp].imag());
+        v = g == 1 ? o : ((i & mp) ? std::complex<double>(0, 1) * o : std::complex<double>(0, -1) * o);
+      }
+      s += std::imag(std::conj(l) * v);
+    }
+    return s;
+  };
   for (int p = 0; p < hdr->npass; ++p) {
     const PassDesc& d = pd[p];
     for (int h = 0; h < d.nphase; ++h) {
       const PhaseDesc& ph = phd[d.phase0 + h];
       auto phys = [&](uint8_t o) -> int { return o >= kFixed ? o - kFixed : d.sbit[ph.rbit[o]]; };
+      if (gen)
+        for (int g = 0; g < ph.ngate; ++g) {
+          const int k = ph.gate0 + g;
+          if (gen[k] && fixed_diag_instr(gi[k])) terms[term[k]] = grad_term(phys(gi[k].a), gen[k]);
+        }
       for (int g = 0; g < ph.ngate; ++g) {
         const GateInstr& G = gi[ph.gate0 + g];
+        if (gen && gen[ph.gate0 + g] && !fixed_diag_instr(G))
+          terms[term[ph.gate0 + g]] = grad_term(phys(G.a), gen[ph.gate0 + g]);
         const C* c = cf + G.coef;
         const int a = phys(G.a);
         const uint64_t ma = 1ull << a;
@@ -772,6 +809,156 @@ static void emulate_t(const uint8_t* prog, std::complex<R>* psi, int n) {
 void emulate_program(const uint8_t* prog, void* state, int n, int dtype) {
   if (dtype == 0) emulate_t<float>(prog, (std::complex<float>*)state, n);
   else emulate_t<double>(prog, (std::complex<double>*)state, n);
+}
+
+}  // namespace qsb
+
+// ---------------------------------------------------------------------------------
+// Adjoint gradient: the reverse sweep as one program over the stacked state
+// ---------------------------------------------------------------------------------
+namespace qsb {
+
+namespace {
+
+// The circuit's gates as U^dagger in reverse order, at physical bits q + 1.
+std::vector<QOp> reverse_ops(const std::vector<GradOp>& fwd) {
+  std::vector<QOp> r;
+  r.reserve(fwd.size());
+  for (size_t k = fwd.size(); k-- > 0;) {
+    const QOp& o = fwd[k].op;
+    QOp d;
+    d.arity = o.arity;
+    d.q0 = o.q0 + 1;
+    d.q1 = o.arity == 2 ? o.q1 + 1 : -1;
+    const int dd = o.arity == 1 ? 2 : 4;
+    for (int i = 0; i < dd; ++i)
+      for (int j = 0; j < dd; ++j) d.U[i * dd + j] = std::conj(o.U[j * dd + i]);
+    r.push_back(d);
+  }
+  return r;
+}
+
+// Classes of the reverse gates.  A parameterised X or Y rotation stays a register gate even
+// where its matrix is diagonal (theta = 0): its gradient term pairs amplitudes across its bit.
+std::vector<COp> classify_grad(const std::vector<QOp>& rev, const std::vector<GradOp>& fwd) {
+  std::vector<COp> c;
+  c.reserve(rev.size());
+  const size_t N = fwd.size();
+  for (size_t i = 0; i < N; ++i) {
+    COp o = classify(rev[i]);
+    const int g = fwd[N - 1 - i].gen;
+    if (g == 1 || g == 2) o.need |= bit(rev[i].q0);
+    c.push_back(o);
+  }
+  return c;
+}
+
+PlanConfig grad_cfg(const PlanConfig& cfg) {
+  PlanConfig pc = cfg;
+  pc.pair_bit = true;  // the lam bit is a register bit of every phase
+  return pc;
+}
+
+}  // namespace
+
+uint64_t grad_signature(const std::vector<GradOp>& fwd, int n, const PlanConfig& cfg) {
+  const std::vector<COp> c = classify_grad(reverse_ops(fwd), fwd);
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&h](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+  mix((uint64_t)n); mix((uint64_t)cfg.m); mix((uint64_t)cfg.r); mix((uint64_t)cfg.k);
+  mix((uint64_t)cfg.hill_iters); mix((uint64_t)cfg.lookahead);
+  for (const COp& o : c) {
+    mix(((uint64_t)o.kind << 16) | ((uint64_t)(o.a & 0xff) << 8) | (uint64_t)(o.b & 0xff));
+    mix(o.need);
+  }
+  for (const GradOp& g : fwd) mix((uint64_t)g.gen);
+  return h;
+}
+
+std::vector<PlannedPass> plan_grad_passes(const std::vector<GradOp>& fwd, int n, const PlanConfig& cfg,
+                                          uint64_t* signature) {
+  const std::vector<COp> c = classify_grad(reverse_ops(fwd), fwd);
+  std::vector<PlannedPass> passes = plan_passes(c, n + 1, grad_cfg(cfg));
+  for (const PlannedPass& ps : passes) {
+    if (ps.sbits.empty() || ps.sbits[0] != 0 || !ps.store_src.empty())
+      throw std::runtime_error("gradient planner: a pass does not stage the lam bit");
+    for (const PlannedPhase& ph : ps.phases)
+      if (std::find(ph.rbits.begin(), ph.rbits.end(), 0) == ph.rbits.end())
+        throw std::runtime_error("gradient planner: a phase does not hold the lam bit in registers");
+  }
+  if (signature) *signature = grad_signature(fwd, n, cfg);
+  return passes;
+}
+
+bool grad_plan_fits(const std::vector<GradOp>& fwd, const std::vector<PlannedPass>& passes) {
+  const std::vector<COp> c = classify_grad(reverse_ops(fwd), fwd);
+  size_t seen = 0;
+  for (const PlannedPass& ps : passes)
+    for (const PlannedPhase& ph : ps.phases) {
+      uint64_t R = 0;
+      for (int j : ph.rbits) R |= bit(ps.sbits[j]);
+      for (int oi : ph.ops) {
+        if (oi < 0 || (size_t)oi >= c.size() || (c[oi].need & ~R)) return false;
+        ++seen;
+      }
+    }
+  return seen == c.size();
+}
+
+GradProgram build_grad_program(const std::vector<GradOp>& fwd, int n, const std::vector<PlannedPass>& passes,
+                               int r) {
+  std::vector<QOp> rev = reverse_ops(fwd);
+  const std::vector<QOp> orig = rev;
+  // scalar extraction with unit-modulus diagonals: the per-thread factors of diagonal gates
+  // on fixed bits (applied wherever the kernel places them in their phase) leave magnitudes
+  // alone, so a term's weight only depends on the register gates before it
+  for (const PlannedPass& ps : passes) extract_pass_scalars(rev, ps.ops, false);
+  const std::vector<COp> c = classify_grad(rev, fwd);
+  GradProgram g;
+  g.prog = encode_program(passes, c, n + 1, 0, r);
+  const size_t N = fwd.size();
+  // squared magnitude of the scalar each gate's rewrite took out
+  std::vector<double> r2(N, 1.0);
+  for (size_t i = 0; i < N; ++i) {
+    const int d = rev[i].arity == 1 ? 2 : 4;
+    int e = 0;
+    for (int k = 1; k < d * d; ++k)
+      if (std::abs(rev[i].U[k]) > std::abs(rev[i].U[e])) e = k;
+    if (std::abs(rev[i].U[e]) > 0.0) r2[i] = std::norm(orig[i].U[e]) / std::norm(rev[i].U[e]);
+  }
+  const ProgramHeader* hdr = (const ProgramHeader*)g.prog.bytes.data();
+  const GateInstr* gi = (const GateInstr*)(g.prog.bytes.data() + hdr->off_gate);
+  g.prog.grad_gen.assign(hdr->ngate, 0);
+  g.prog.grad_term.assign(hdr->ngate, -1);
+  double f2 = 1.0;  // |actual / carried|^2 of both halves before the current instruction
+  int k = 0;
+  for (const PlannedPass& ps : passes)
+    for (const PlannedPhase& ph : ps.phases) {
+      const double start = f2;
+      for (int oi : ph.ops) {
+        const GradOp& src = fwd[N - 1 - (size_t)oi];
+        const bool hoisted = fixed_diag_instr(gi[k]);
+        if (hoisted && std::abs(r2[oi] - 1.0) > 1e-9)
+          throw std::runtime_error("gradient program: a diagonal gate on fixed bits rescales the state");
+        if (src.gen) {
+          if (src.op.arity != 1) throw std::runtime_error("gradient program: parameterised gates are single-qubit");
+          g.prog.grad_gen[k] = (int8_t)src.gen;
+          g.prog.grad_term[k] = g.prog.nterm++;
+          g.term_slot.push_back(src.slot);
+          g.term_w.push_back(hoisted ? start : f2);
+        }
+        f2 *= r2[oi];
+        ++k;
+      }
+    }
+  if (k != hdr->ngate) throw std::runtime_error("gradient program: instruction count mismatch");
+  return g;
+}
+
+void emulate_grad_program(const GradProgram& g, void* phi, double* terms) {
+  const ProgramHeader* hdr = (const ProgramHeader*)g.prog.bytes.data();
+  emulate_t<float>(g.prog.bytes.data(), (std::complex<float>*)phi, hdr->n, g.prog.grad_gen.data(),
+                   g.prog.grad_term.data(), terms);
 }
 
 }  // namespace qsb

@@ -35,7 +35,9 @@ COp classify(const QOp& op);
 // Rewrites the gates of one planned pass as s * V (one entry of V exactly 1, as many
 // entries as possible in {0, +-1, +-i}) and multiplies the product of the scalars into one
 // gate of the pass.  The classification (need/touch bits) of every gate is unchanged.
-void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops);
+// diag_absorbs = false: diagonal gates never absorb the product (they keep unit-modulus
+// entries); a pass of diagonal gates only then drops its product, a unit-modulus phase.
+void extract_pass_scalars(std::vector<QOp>& ops, const std::vector<int>& pass_ops, bool diag_absorbs = true);
 
 struct PlanConfig {
   int m = 13;             // local bits per pass
@@ -79,6 +81,13 @@ struct Program {
   int threads = 0;        // block size (max over passes of 2^(m - r))
   size_t max_smem = 0;    // bytes of shared memory per block
   bool has_gates = false;  // at least one gate instruction
+  // Gradient programs only (the reverse sweep of an adjoint gradient over the stacked state
+  // psi (+) lam, physical bit 0 selecting lam; empty otherwise), per gate instruction: the
+  // generator of a parameterised rotation (0 none, 1 X, 2 Y, 3 Z) and the index of its
+  // gradient term Im <lam|G|psi> (-1 none).  Terms are numbered in instruction order.
+  std::vector<int8_t> grad_gen;
+  std::vector<int32_t> grad_term;
+  int nterm = 0;
 };
 
 // r_req: register bits per thread (the generic kernel's fixed value when <= 0:
@@ -92,5 +101,41 @@ Program build_program(std::vector<QOp>& ops, const std::vector<PlannedPass>& pas
 
 // Reference interpretation of a program on host memory (used by CPU tests of the planner).
 void emulate_program(const uint8_t* prog, void* state, int n, int dtype);
+
+// ---- adjoint gradient over the stacked state -------------------------------------------
+// A gate of the forward circuit (qubit indices = bit positions of the n-qubit state) with
+// its parameter: gen 0 none, 1 X, 2 Y, 3 Z (R(theta) = exp(-i theta G / 2)), slot = index of
+// dE/dtheta.
+struct GradOp {
+  QOp op;
+  int gen = 0, slot = -1;
+};
+
+// Reverse-sweep program over Phi = psi (+) lam on n + 1 qubits (physical bit 0 selects lam,
+// circuit qubit q is physical bit q + 1): the circuit's gates as U^dagger in reverse order;
+// before each parameterised gate its term Im <lam|G|psi> is accumulated, term t weighing
+// term_w[t] (the squared magnitude of the scalars extracted before it) into gradient slot
+// term_slot[t].
+struct GradProgram {
+  Program prog;
+  std::vector<int> term_slot;
+  std::vector<double> term_w;
+};
+
+// Planned passes of the reverse sweep (gate classes and bits only: reusable for any
+// parameter values of the same structure) and the structure's signature.
+std::vector<PlannedPass> plan_grad_passes(const std::vector<GradOp>& fwd, int n, const PlanConfig& cfg,
+                                          uint64_t* signature);
+uint64_t grad_signature(const std::vector<GradOp>& fwd, int n, const PlanConfig& cfg);
+// Whether a plan made for other matrix values of the same circuit holds these values' gates
+// (every gate's register needs met in its phase).
+bool grad_plan_fits(const std::vector<GradOp>& fwd, const std::vector<PlannedPass>& passes);
+GradProgram build_grad_program(const std::vector<GradOp>& fwd, int n, const std::vector<PlannedPass>& passes,
+                               int r);
+
+// Host interpretation of a gradient program on Phi (complex64, 2^(n+1) amplitudes, the
+// program's own coefficients): terms[t] (FP64, unweighted) as the specialised kernels
+// accumulate them.
+void emulate_grad_program(const GradProgram& g, void* phi, double* terms);
 
 }  // namespace qsb

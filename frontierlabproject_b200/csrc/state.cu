@@ -980,6 +980,338 @@ int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nop
   });
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------
+// Adjoint gradient with the specialised kernels: forward tile, stacked observable, one
+// reverse program over Phi = psi (+) H psi
+// ------------------------------------------------------------------------------------
+namespace {
+
+std::vector<GradOp> read_grad_ops(const qs_adj_op* ops, int nops, int n, int nparams) {
+  if (nops < 0 || (nops > 0 && !ops)) throw InvalidArg{"gradient: null ops"};
+  std::vector<GradOp> out(nops);
+  for (int i = 0; i < nops; ++i) {
+    const qs_adj_op& o = ops[i];
+    GradOp& g = out[i];
+    if (!o.U) throw InvalidArg{"gradient: null gate matrix"};
+    if (o.kind == QS_OP_1Q) {
+      if (o.q0 < 0 || o.q0 >= n) throw InvalidArg{"gradient: invalid q0"};
+      if (o.gen < 0 || o.gen > 3) throw InvalidArg{"gradient: generator must be 0..3"};
+      if (o.gen && (o.grad_index < 0 || o.grad_index >= nparams)) throw InvalidArg{"gradient: grad_index out of range"};
+      g.op.arity = 1;
+      g.op.q0 = o.q0;
+      for (int e = 0; e < 4; ++e) g.op.U[e] = cplx(o.U[2 * e], o.U[2 * e + 1]);
+      g.gen = o.gen;
+      g.slot = o.gen ? o.grad_index : -1;
+    } else if (o.kind == QS_OP_2Q) {
+      if (o.q0 < 0 || o.q0 >= n || o.q1 < 0 || o.q1 >= n || o.q0 == o.q1) throw InvalidArg{"gradient: invalid q0/q1"};
+      if (o.gen != 0) throw InvalidArg{"gradient: two-qubit gates carry no parameter"};
+      g.op.arity = 2;
+      g.op.q0 = o.q0;
+      g.op.q1 = o.q1;
+      for (int e = 0; e < 16; ++e) g.op.U[e] = cplx(o.U[2 * e], o.U[2 * e + 1]);
+    } else {
+      throw InvalidArg{"gradient: unknown op kind: " + std::to_string(o.kind)};
+    }
+  }
+  return out;
+}
+
+bool same_grad_structure(const std::vector<GradOp>& a, const std::vector<GradOp>& b) {
+  if (a.size() != b.size()) return false;
+  for (size_t i = 0; i < a.size(); ++i)
+    if (a[i].op.arity != b[i].op.arity || a[i].op.q0 != b[i].op.q0 || a[i].op.q1 != b[i].op.q1 ||
+        a[i].gen != b[i].gen || a[i].slot != b[i].slot)
+      return false;
+  return true;
+}
+
+PlanConfig grad_plan_cfg(int n, const qs_config* c) {
+  PlanConfig p;
+  p.r = 5;
+  p.m = c && c->m > 0 ? c->m : 13;
+  p.k = c && c->k > 0 ? c->k : 3;
+  p.hill_iters = c ? c->hill_iters : 16;
+  p.m = std::max(p.r, std::min(p.m, n + 1));
+  return p;
+}
+
+}  // namespace
+
+struct qs_grad {
+  int n = 0, nparams = 0;
+  std::vector<GradOp> structure;
+  qs_state* fwd = nullptr;        // the forward state (n qubits), specialised kernels
+  PlanConfig pc;
+  std::vector<PlannedPass> rplan;  // reverse program (n + 1 qubits)
+  void* phi = nullptr;             // stacked state, 2^(n+1) complex64
+  uint8_t* d_prog = nullptr;
+  size_t prog_cap = 0;
+  uint8_t* h_prog = nullptr;       // pinned staging of the reverse program
+  size_t hprog_cap = 0;
+  double* d_out = nullptr;         // energy, then the terms
+  double* h_out = nullptr;         // pinned
+  size_t out_cap = 0;
+  GraphEntry graph;
+  int rev_phases = 0, nterm = 0, fwd_sweeps = 0;
+
+  ~qs_grad() {
+    if (fwd) cudaStreamSynchronize(fwd->stream);
+    if (graph.exec) cudaGraphExecDestroy(graph.exec);
+    if (phi) cudaFree(phi);
+    if (d_prog) cudaFree(d_prog);
+    if (h_prog) cudaFreeHost(h_prog);
+    if (d_out) cudaFree(d_out);
+    if (h_out) cudaFreeHost(h_out);
+    delete fwd;
+  }
+
+  void run(const std::vector<GradOp>& f, const double* a, const double* b, double* energy, double* grads) {
+    qs_state* s = fwd;
+    cudaStream_t st = s->stream;
+    // forward: psi = U|0>, one graphed tile of the specialised kernels
+    s->queue.clear();
+    for (int p = 0; p < n; ++p) s->pos2bit[p] = p;
+    CK(launch_set_basis(0, s->psi, n, 0, st));
+    std::vector<QOp> q;
+    q.reserve(f.size());
+    for (const GradOp& g : f) q.push_back(g.op);
+    const unsigned long long sw0 = s->st.sweeps;
+    enqueue(s, std::move(q), QS_MODE_GRAPHED);
+    s->flush();
+    fwd_sweeps = (int)(s->st.sweeps - sw0);
+    if (!grads) {  // energy only
+      CK(cudaMemsetAsync(s->d_acc, 0, sizeof(double), st));
+      CK(launch_zz_x_stack(s->psi, phi, n, a, b, s->d_acc, st));
+      s->st.launches += 1;
+      CK(cudaMemcpyAsync(s->h_acc, s->d_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      s->check_device_error();
+      *energy = s->h_acc[0];
+      return;
+    }
+    // reverse program (host): scalar extraction for these values, encoding, term weights; a
+    // gate whose class changed with its values (a diagonal became dense) takes a new plan
+    if (!grad_plan_fits(f, rplan)) {
+      rplan = plan_grad_passes(f, n, pc, nullptr);
+      rev_phases = 0;
+      for (const PlannedPass& ps : rplan) rev_phases += (int)ps.phases.size();
+    }
+    GradProgram gp = build_grad_program(f, n, rplan, pc.r);
+    nterm = gp.prog.nterm;
+    const size_t outb = (size_t)(1 + nterm) * sizeof(double);
+    if (outb > out_cap) {
+      CK(cudaStreamSynchronize(st));
+      if (d_out) CK(cudaFree(d_out));
+      if (h_out) CK(cudaFreeHost(h_out));
+      d_out = nullptr;
+      h_out = nullptr;
+      out_cap = 0;
+      CK(dev_malloc((void**)&d_out, outb));
+      CK(host_malloc((void**)&h_out, outb));
+      out_cap = outb;
+      if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
+    }
+    const size_t pb = gp.prog.bytes.size();
+    if (pb > prog_cap || pb > hprog_cap) {
+      CK(cudaStreamSynchronize(st));
+      if (d_prog) CK(cudaFree(d_prog));
+      if (h_prog) CK(cudaFreeHost(h_prog));
+      d_prog = nullptr;
+      h_prog = nullptr;
+      prog_cap = hprog_cap = 0;
+      CK(dev_malloc((void**)&d_prog, pb * 2));
+      CK(host_malloc((void**)&h_prog, pb * 2));
+      prog_cap = hprog_cap = pb * 2;
+      if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
+    }
+    std::memcpy(h_prog, gp.prog.bytes.data(), pb);  // the previous run's copy has completed (run ends synchronised)
+    CK(cudaMemcpyAsync(d_prog, h_prog, pb, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(d_out, 0, outb, st));
+    // Phi = psi (+) H psi and the energy
+    CK(launch_zz_x_stack(s->psi, phi, n, a, b, d_out, st));
+    s->st.launches += 1;
+    // the reverse program: one launch per pass, captured as a graph (parameter values only
+    // update it)
+    JitConfig jc;
+    jc.blocks = 2;
+    jc.packed = false;
+    std::shared_ptr<JitKernels> jk = jit_get(gp.prog, jc);
+    s->st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
+    s->st.jit_modules += (unsigned long long)jk->chunks;
+    s->st.jit_disk_hits += (unsigned long long)jk->disk_hits;
+    jk->compile_seconds = 0.0;
+    jk->chunks = 0;
+    jk->disk_hits = 0;
+    const uint64_t key = jk->key ^ ((uint64_t)(uintptr_t)phi * 0x9E3779B97F4A7C15ull) ^
+                         ((uint64_t)(uintptr_t)d_prog << 1) ^ ((uint64_t)(uintptr_t)d_out << 3);
+    const uint64_t values = coef_values_hash(gp.prog);
+    const uint8_t* host_coef = gp.prog.bytes.data() + ((const ProgramHeader*)gp.prog.bytes.data())->off_coef;
+    auto capture = [&]() {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = cudaSuccess;
+      for (int p = 0; p < gp.prog.npass && e == cudaSuccess; ++p)
+        e = jit_launch(*jk, p, d_prog, host_coef, phi, s->d_ctl + 2, gp.prog.threads, gp.prog.max_smem,
+                       device_sm_count(), st, d_out + 1);
+      cudaError_t e2 = cudaStreamEndCapture(st, &g);
+      if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
+      if (e2 != cudaSuccess) throw CudaError{e2};
+      return g;
+    };
+    bool updated = false;
+    if (graph.exec && graph.key == key && graph.values != values) {
+      cudaGraph_t g = capture();
+      cudaGraphExecUpdateResultInfo info;
+      const cudaError_t eu = cudaGraphExecUpdate(graph.exec, g, &info);
+      cudaGraphDestroy(g);
+      if (eu == cudaSuccess) {
+        graph.values = values;
+        updated = true;
+      } else {
+        cudaGetLastError();
+        CK(cudaGraphExecDestroy(graph.exec));
+        graph.exec = nullptr;
+      }
+    }
+    if (!graph.exec || graph.key != key) {
+      if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
+      graph.kernels = jk;
+      cudaGraph_t g = capture();
+      cudaError_t e3 = cudaGraphInstantiate(&graph.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e3 != cudaSuccess) throw CudaError{e3};
+      graph.key = key;
+      graph.values = values;
+      s->st.graph_builds += 1;
+    } else if (updated) {
+      s->st.graph_builds += 1;
+    } else {
+      s->st.graph_replays += 1;
+    }
+    CK(cudaGraphLaunch(graph.exec, st));
+    s->st.launches += 1;
+    s->st.sweeps += gp.prog.npass;
+    CK(cudaMemcpyAsync(h_out, d_out, outb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    s->check_device_error();
+    *energy = h_out[0];
+    for (int k = 0; k < nparams; ++k) grads[k] = 0.0;
+    for (int t = 0; t < nterm; ++t) grads[gp.term_slot[t]] += gp.term_w[t] * h_out[1 + t];
+  }
+};
+
+extern "C" {
+
+int qs_grad_create(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                   qs_grad** out) {
+  return guard([&] {
+    if (!out) throw InvalidArg{"null output handle"};
+    *out = nullptr;
+    if (num_qubits < 10 || num_qubits > 33) throw InvalidArg{"gradient: num_qubits must be in [10, 33]"};
+    if (nparams < 0) throw InvalidArg{"gradient: nparams < 0"};
+    std::string why;
+    if (!jit_available(&why)) throw InvalidArg{"gradient: specialised kernels unavailable: " + why};
+    std::unique_ptr<qs_grad> g(new qs_grad());
+    g->n = num_qubits;
+    g->nparams = nparams;
+    g->structure = read_grad_ops(ops, nops, num_qubits, nparams);
+    g->pc = grad_plan_cfg(num_qubits, cfg);
+    g->rplan = plan_grad_passes(g->structure, num_qubits, g->pc, nullptr);
+    for (const PlannedPass& ps : g->rplan) g->rev_phases += (int)ps.phases.size();
+    qs_state* s = nullptr;
+    const int rc = qs_create(num_qubits, QS_C64, &s);
+    if (rc != 0) throw InvalidArg{std::string(qs_last_error())};
+    g->fwd = s;
+    s->jit_mode = 1;
+    if (cfg) {
+      if (cfg->m > 0) s->cfg.m = std::min(cfg->m, 13);
+      if (cfg->k > 0) s->cfg.k = cfg->k;
+      s->cfg.hill_iters = cfg->hill_iters;
+    }
+    CK(dev_malloc(&g->phi, (sizeof(float) * 2) << (num_qubits + 1)));
+    *out = g.release();
+  });
+}
+
+int qs_grad_run(qs_grad* g, const qs_adj_op* ops, int nops, const double* a, const double* b, double* energy,
+                double* grads) {
+  return guard([&] {
+    if (!g || !a || !b || !energy) throw InvalidArg{"null argument"};
+    std::vector<GradOp> f = read_grad_ops(ops, nops, g->n, g->nparams);
+    if (!same_grad_structure(f, g->structure))
+      throw InvalidArg{"gradient: the circuit's structure differs from the one the handle was created for"};
+    g->run(f, a, b, energy, grads);
+  });
+}
+
+int qs_grad_info(const qs_grad* g, int* fwd_sweeps, int* rev_sweeps, int* rev_phases, int* terms) {
+  return guard([&] {
+    if (!g) throw InvalidArg{"null handle"};
+    if (fwd_sweeps) *fwd_sweeps = g->fwd_sweeps;
+    if (rev_sweeps) *rev_sweeps = (int)g->rplan.size();
+    if (rev_phases) *rev_phases = g->rev_phases;
+    if (terms) *terms = g->nterm;
+  });
+}
+
+int qs_grad_stats(qs_grad* g, qs_stats* out) {
+  return guard([&] {
+    if (!g || !out) throw InvalidArg{"null argument"};
+    *out = g->fwd->st;
+  });
+}
+
+int qs_grad_destroy(qs_grad* g) {
+  return guard([&] { delete g; });
+}
+
+int qs_grad_jit_check(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                      int* sweeps, char* logbuf, int logcap) {
+  return guard([&] {
+    if (num_qubits < 10 || num_qubits > 33) throw InvalidArg{"gradient: num_qubits must be in [10, 33]"};
+    std::vector<GradOp> f = read_grad_ops(ops, nops, num_qubits, nparams);
+    const PlanConfig pc = grad_plan_cfg(num_qubits, cfg);
+    std::vector<PlannedPass> passes = plan_grad_passes(f, num_qubits, pc, nullptr);
+    GradProgram gp = build_grad_program(f, num_qubits, passes, pc.r);
+    JitConfig jc;
+    jc.blocks = 2;
+    jc.packed = false;
+    std::string log;
+    const bool ok = jit_compile_check(gp.prog, &log, jc);
+    if (logbuf && logcap > 0) {
+      const size_t k = std::min<size_t>(log.size(), (size_t)logcap - 1);
+      std::memcpy(logbuf, log.data(), k);
+      logbuf[k] = '\0';
+    }
+    if (!ok) throw InvalidArg{"jit compile failed:\n" + log.substr(0, 4000)};
+    if (sweeps) *sweeps = gp.prog.npass;
+  });
+}
+
+int qs_grad_emulate(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                    const void* psi, const void* lam, double* grads) {
+  return guard([&] {
+    if (!psi || !lam || (nparams > 0 && !grads)) throw InvalidArg{"null argument"};
+    if (num_qubits < 10 || num_qubits > 22) throw InvalidArg{"gradient emulation: num_qubits must be in [10, 22]"};
+    std::vector<GradOp> f = read_grad_ops(ops, nops, num_qubits, nparams);
+    const PlanConfig pc = grad_plan_cfg(num_qubits, cfg);
+    std::vector<PlannedPass> passes = plan_grad_passes(f, num_qubits, pc, nullptr);
+    if (!grad_plan_fits(f, passes)) throw InvalidArg{"gradient emulation: plan does not hold the gates"};
+    GradProgram gp = build_grad_program(f, num_qubits, passes, pc.r);
+    const uint64_t dim = 1ull << num_qubits;
+    std::vector<std::complex<float>> phi(2 * dim);
+    const std::complex<float>* ps = (const std::complex<float>*)psi;
+    const std::complex<float>* ls = (const std::complex<float>*)lam;
+    for (uint64_t x = 0; x < dim; ++x) { phi[2 * x] = ps[x]; phi[2 * x + 1] = ls[x]; }
+    std::vector<double> terms(std::max(1, gp.prog.nterm), 0.0);
+    emulate_grad_program(gp, phi.data(), terms.data());
+    for (int k = 0; k < nparams; ++k) grads[k] = 0.0;
+    for (int t = 0; t < gp.prog.nterm; ++t) grads[gp.term_slot[t]] += gp.term_w[t] * terms[t];
+  });
+}
+
 int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream) {
   return guard([&] {
     if (!psi || !U) throw InvalidArg{"null argument"};
@@ -1038,6 +1370,7 @@ int qs_plan_info(int num_qubits, int dtype, const qs_op* ops, int nops, const qs
     PlanConfig pc = cfg_from(dtype, num_qubits, cfg);
     // complex64 with an explicit register-bit count: plan as the specialised kernels would
     if (dtype == 0 && cfg && cfg->jit_lr >= 3 && cfg->jit_lr <= 6) pc.r = cfg->jit_lr;
+    pc.pair_bit = dtype == 0 && cfg && cfg->jit_packed == 1;
     auto passes = plan_passes(c, num_qubits, pc);
     int ph = 0;
     for (auto& p : passes) ph += (int)p.phases.size();

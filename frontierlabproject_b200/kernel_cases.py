@@ -12,6 +12,9 @@ Cases and the kernels they launch:
   perm      pass_kernel<float>  in-place permutation passes (a random layout materialised)
   gate      gate1/gate2_kernel  one sweep per gate (sequential mode: the plain method)
   adjoint   adjoint_gate1/2, zz_x_kernel   per-gate adjoint sweep (method="per_gate")
+  gradient  qp_<key>_<p>        the jit gradient of one ansatz (n qubits, 20 layers): forward tile,
+                                zz_x stack kernel, reverse program over the stacked state
+  gradient_batch  batch_kernel  the same gradient as one persistent batched launch (method="fused")
   batch     batch_kernel        one persistent launch of a batched variational workload
   sample    sample_* kernels    measurement sampling
   dense6    dense6_tc_pipe_kernel    tensor-core 64x64 unitary on positions 0..5
@@ -123,6 +126,39 @@ def case_adjoint(n, reps):
             "reverse_launches_per_run": len(pc.gates), "bytes_per_reverse_launch": 4 * (1 << n) * 8}
 
 
+def _gradient(n, reps, method):
+    import torch
+    from . import circuits as C
+    from .adjoint import AdjointEngine, ParamCircuit
+    pc = ParamCircuit.hea(n, 20)
+    th = np.random.default_rng(0).uniform(-np.pi, np.pi, pc.num_params)
+    a, b = C.hea_observable(n, 1)
+    eng = AdjointEngine(n, f32=True, method=method)
+    eng.energy_and_grad(pc, th, a, b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        eng.energy_and_grad(pc, th, a, b)
+    torch.cuda.synchronize()
+    out = {"seconds_per_gradient_wall": (time.perf_counter() - t0) / reps, "parameters": pc.num_params,
+           "gates": len(pc.gates)}
+    if method == "jit":
+        out["engine"] = eng.info()
+    return out
+
+
+def case_gradient(n, reps):
+    out = _gradient(n, reps, "jit")
+    out["kernel"] = "qp_<key>_<p> (forward tile and reverse program), zz_x_kernel<float2,true>"
+    return out
+
+
+def case_gradient_batch(n, reps):
+    out = _gradient(n, reps, "fused")
+    out["kernel"] = "batch_kernel<256> (one instance)"
+    return out
+
+
 def case_batch(n, reps):
     from .batch import BatchedAdjoint, BatchShape, hea_batch
     insts = hea_batch(48, n_range=(12, min(n, 20)), l_range=(4, 8), seed=0)
@@ -178,7 +214,9 @@ def case_reduce(n, reps):
     return {"kernel": "inner_kernel", "seconds_per_call": t, "bytes_per_call": 2 * (1 << n) * 8}
 
 
-CASES = {"pass": case_pass, "perm": case_perm, "gate": case_gate, "adjoint": case_adjoint, "batch": case_batch,
+CASES = {"pass": case_pass, "perm": case_perm, "gate": case_gate, "adjoint": case_adjoint, "gradient": case_gradient,
+         "gradient_batch": case_gradient_batch,
+         "batch": case_batch,
          "sample": case_sample, "dense6": case_dense6, "dense": case_dense, "reduce": case_reduce}
 
 

@@ -211,6 +211,37 @@ typedef struct {
 QS_API int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, int nops, double* grads,
                             int ngrads);
 
+/* Adjoint gradient with the plan-time specialised kernels (complex64 states, FP64 energy and
+ * gradient; no counterpart in the reference).  psi = U|0...0> runs as one graphed tile; one
+ * kernel then writes the stacked state Phi = psi (+) H psi (n + 1 qubits, Phi[2x] = psi[x],
+ * Phi[2x + 1] = (H psi)[x]) and the energy; the reverse sweep is ONE planned program over Phi
+ * (both states uncomputed by the same U_k^dagger), whose kernels add Im <lam|G|psi> before
+ * each rotation into per-gate FP64 terms.  Plans and kernels follow the circuit's structure
+ * (gate kinds, qubits, generators, slots): new parameter values reuse them.  10 <= n <= 33.
+ * cfg (optional): m, k and hill_iters of the plans (other fields ignored). */
+typedef struct qs_grad qs_grad;
+QS_API int qs_grad_create(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                          qs_grad** out);
+/* Same structure as at creation, any matrices: energy and grads (nparams doubles, overwritten;
+ * NULL: the energy only, no reverse sweep).  QS_ERR_INVALID when the structure differs. */
+QS_API int qs_grad_run(qs_grad* g, const qs_adj_op* ops, int nops, const double* a, const double* b, double* energy,
+                       double* grads);
+/* Sweeps of the last forward run and of the reverse program, register phases of the
+ * reverse program, gradient terms (one per rotation). */
+QS_API int qs_grad_info(const qs_grad* g, int* fwd_sweeps, int* rev_sweeps, int* rev_phases, int* terms);
+/* Execution counters of the handle (launches, sweeps, graph builds, kernel compiles). */
+QS_API int qs_grad_stats(qs_grad* g, qs_stats* out);
+QS_API int qs_grad_destroy(qs_grad* g);
+/* Compiles the reverse program's kernels on the host only (NVRTC; tests): sweeps and the
+ * compiler's resource log (registers, spills) in logbuf. */
+QS_API int qs_grad_jit_check(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                             int* sweeps, char* logbuf, int logcap);
+/* Host interpretation of the reverse program (CPU tests of its planning, scalar weights and
+ * term placement): psi = U|0> and lam = H psi given (complex64, 2^n each), grads out.
+ * 10 <= n <= 22. */
+QS_API int qs_grad_emulate(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
+                           const void* psi, const void* lam, double* grads);
+
 /* Module-level apply_1q_gate / apply_2q_gate (bindings.cpp:931-1001): gate on a raw
  * device array psi of 2^num_qubits amplitudes; U is a host matrix; stream may be NULL. */
 QS_API int qs_apply_1q_gate(void* psi, int dtype, const void* U, int target_qubit, int num_qubits, void* stream);
@@ -349,6 +380,9 @@ QS_API int qs_batch_run(qs_batch* b, void* stream, float* ms);
 QS_API int qs_batch_results(qs_batch* b, double* energies, double* grads);
 QS_API int qs_batch_info(const qs_batch* b, int* nitems, int* nparams_total, long long* arena_bytes, int* grid);
 QS_API int qs_batch_destroy(qs_batch* b);
+/* Host-side plan of a batch (no device work): per instance five ints in stats[5 * i ..]:
+ * passes, passes run in register phases, register phases, gates, work items. */
+QS_API int qs_batch_describe(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, int* stats);
 /* Host emulation of the same device program (items in list order, FP64 states): tests of
  * the batch planner and encoder without a GPU. */
 QS_API int qs_batch_emulate(const qs_batch_instance* insts, int ninst, const qs_batch_config* cfg, double* energies,

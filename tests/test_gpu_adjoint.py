@@ -71,21 +71,36 @@ def test_torch_autograd():
     assert np.allclose(t.grad.numpy(), 2.0 * g_ref, atol=1e-10)
 
 
-def test_config3_full_size_c64_vs_c128_and_finite_differences():
-    # the benchmark workload itself: n = 24, L = 20 (960 parameters, 1440 gates), complex64
-    # states with FP64 accumulation (one persistent launch) against the complex128 adjoint, and
-    # the complex128 gradient against central finite differences (h = 1e-3) on 8 parameters
+@pytest.fixture(scope="module")
+def config3():
+    # the benchmark workload itself: n = 24, L = 20 (960 parameters, 1440 gates); the complex128
+    # adjoint (per-gate reverse sweep) is the reference
     from frontierlabproject_b200.adjoint import AdjointEngine
     n, L = 24, 20
     pc, th, a, b = _case(n, L, 0)
     assert pc.num_params == 960
-    eng32 = AdjointEngine(n, f32=True)
-    E32, g32 = eng32.energy_and_grad(pc, th, a, b)
-    assert eng32.method == "fused"
     eng64 = AdjointEngine(n, f32=False)
     E64, g64 = eng64.energy_and_grad(pc, th, a, b)
+    return pc, th, a, b, eng64, E64, g64
+
+
+@pytest.mark.parametrize("method", ["jit", "fused"])
+def test_config3_full_size_c64_vs_c128(config3, method):
+    # complex64 states with FP64 accumulation: the specialised-kernel program over the stacked
+    # state (jit, the default at this size) and the batched persistent launch (fused)
+    from frontierlabproject_b200.adjoint import AdjointEngine
+    pc, th, a, b, _, E64, g64 = config3
+    eng32 = AdjointEngine(24, f32=True, method=method)
+    E32, g32 = eng32.energy_and_grad(pc, th, a, b)
+    assert eng32.method == method
     assert np.linalg.norm(g32 - g64) <= 1e-5 * np.linalg.norm(g64)
     assert abs(E32 - E64) <= 1e-5 * max(1.0, abs(E64))
+    assert AdjointEngine(24, f32=True).method == "jit"
+
+
+def test_config3_c128_vs_finite_differences(config3):
+    # the complex128 gradient against central finite differences (h = 1e-3) on 8 parameters
+    pc, th, a, b, eng64, _, g64 = config3
     h = 1e-3
     for k in (0, 1, 137, 480, 481, 700, 958, 959):
         tp, tm = th.copy(), th.copy()
