@@ -282,7 +282,7 @@ def adjoint_bench(n: int = 24, layers: int = 20, reps: int = 10, seed: int = 0) 
     for _ in range(k):
         eng.energy(pc, th, a, b)
     t_e = (time.perf_counter() - t0) / k
-    plain = AdjointEngine(n, f32=True, mode="sequential")
+    plain = AdjointEngine(n, f32=True, mode="sequential", method="per_gate")
     plain.energy(pc, th, a, b)
     t0 = time.perf_counter()
     plain.energy(pc, th, a, b)

@@ -160,6 +160,7 @@ class AdjointEngine:
         self._np_dtype = np.complex64 if f32 else np.complex128
         self._fused = None      # (structure key, BatchedAdjoint)
         self._grad = None       # (structure key, qs_grad handle, AdjOps)
+        self._grad_cfg = None   # plan knobs of the jit method
 
     def __del__(self):
         g = getattr(self, "_grad", None)
@@ -171,8 +172,17 @@ class AdjointEngine:
             self._grad = None
 
     def set_config(self, **kw) -> None:
+        """Executor knobs (``StatevectorF32.set_config``); the jit method takes ``m``, ``k``,
+        ``hill_iters`` and ``jit_lr`` (5 or 6) for its plans (applied to the next handle)."""
         if self.method == "jit":
-            raise ValueError("the jit gradient plans with its own configuration")
+            allowed = {"m", "k", "hill_iters", "jit_lr"}
+            if set(kw) - allowed:
+                raise ValueError(f"the jit gradient takes only {sorted(allowed)}")
+            self._grad_cfg = dict(self._grad_cfg or {}, **kw)
+            if self._grad is not None:
+                N.lib().qs_grad_destroy(self._grad[1])
+                self._grad = None
+            return
         self.psi.set_config(**kw)
         self.lam.set_config(**kw)
 
@@ -229,7 +239,13 @@ class AdjointEngine:
             tab = AdjOps(pc)
             ops = tab.update(theta)
             h = ctypes.c_void_p()
-            N.call("qs_grad_create", self.n, ops.ctypes.data, len(ops), pc.num_params, None, ctypes.byref(h))
+            cfg = None
+            if self._grad_cfg:
+                c = N.QsConfig(13, 3, 16, 0, 1, 5, 2, 0)
+                for name, v in self._grad_cfg.items():
+                    setattr(c, name, int(v))
+                cfg = ctypes.byref(c)
+            N.call("qs_grad_create", self.n, ops.ctypes.data, len(ops), pc.num_params, cfg, ctypes.byref(h))
             self._grad = (key, h, tab)
         h, tab = self._grad[1], self._grad[2]
         ops = tab.update(theta)

@@ -684,20 +684,21 @@ void gen_gate(Gen& G, const GateInstr& g, const PassDesc& pd, const PhaseDesc& p
 }
 
 // Gradient programs: before a parameterised gate (generator gen on the instruction's operand),
-// the thread's part of Im <lam|G|psi> over its registers (register bit A holds the lam bit),
-// reduced over the warp and added to the block's term `local` (shared memory, FP64).  A
-// fixed operand only occurs for Z (a diagonal gate): its sign is the thread's bit.  Under a
-// flipped frame bit the registers of the gate's bit hold X-conjugated data: X G X = -G for
-// Y and Z.
-void gen_term(Gen& G, const GateInstr& g, int gen, int local, int A) {
+// the thread's part of Im <lam|G|psi> over its registers (register bit A holds the lam bit)
+// into a phase-scope accumulator gt<local>; the accumulators are reduced over the warp in
+// batches (gen_term_flush: independent shuffle chains).  A fixed operand only occurs for Z (a
+// diagonal gate): its sign is the thread's bit.  Under a flipped frame bit the registers of
+// the gate's bit hold X-conjugated data: X G X = -G for Y and Z.
+void gen_term(Gen& G, const GateInstr& g, int gen, int local, int A, std::vector<int>* pending) {
   auto& o = G.o;
   if (A < 0 || !G.mask[A].empty()) throw std::runtime_error("jit: the lam bit is not a plain register bit");
   const std::string AM = std::to_string(1 << A);
-  o << "{float gv=0.f;";
+  const std::string v = "gt" + std::to_string(local);
+  o << "float " << v << "=0.f;{";
   if (g.a >= kFixed) {
     if (gen != 3) throw std::runtime_error("jit: an X or Y rotation on a fixed bit");
     o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << AM << ")){const float2 p=a[i],l=a[i|" << AM
-      << "];gv+=l.x*p.y-l.y*p.x;}\nif(" << bitcond(g.a - kFixed) << ")gv=-gv;";
+      << "];" << v << "+=l.x*p.y-l.y*p.x;}\nif(" << bitcond(g.a - kFixed) << ")" << v << "=-" << v << ";";
   } else {
     const int J = g.a;
     if (J == A) throw std::runtime_error("jit: a gate on the lam bit");
@@ -705,15 +706,30 @@ void gen_term(Gen& G, const GateInstr& g, int gen, int local, int A) {
     G.masked({J}, [&](unsigned cm) {
       const bool flip = cm != 0 && gen != 1;
       o << "\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << AJ << ")){const float2 p0=a[i],p1=a[i|" << JM
-        << "],l0=a[i|" << AM << "],l1=a[i|" << AJ << "];gv" << (flip ? "-=" : "+=");
+        << "],l0=a[i|" << AM << "],l1=a[i|" << AJ << "];" << v << (flip ? "-=" : "+=");
       if (gen == 1) o << "(l0.x*p1.y-l0.y*p1.x)+(l1.x*p0.y-l1.y*p0.x);}\n";
       else if (gen == 2) o << "(l1.x*p0.x+l1.y*p0.y)-(l0.x*p1.x+l0.y*p1.y);}\n";
       else o << "(l0.x*p0.y-l0.y*p0.x)-(l1.x*p1.y-l1.y*p1.x);}\n";
     });
   }
-  o << "gv+=__shfl_xor_sync(0xffffffffu,gv,16);gv+=__shfl_xor_sync(0xffffffffu,gv,8);"
-    << "gv+=__shfl_xor_sync(0xffffffffu,gv,4);gv+=__shfl_xor_sync(0xffffffffu,gv,2);"
-    << "gv+=__shfl_xor_sync(0xffffffffu,gv,1);if((threadIdx.x&31u)==0u)atomicAdd(ga+" << local << ",(double)gv);}\n";
+  o << "}\n";
+  pending->push_back(local);
+}
+
+// accumulators live at once (registers) before a flush
+constexpr int kTermBatch = 4;
+
+// Warp sums of the pending term accumulators, interleaved per shuffle distance; lane 0 adds
+// them to its warp's row of the block's terms (no shared-memory atomics: one writer per row).
+void gen_term_flush(Gen& G, std::vector<int>* pending, int nt) {
+  if (pending->empty()) return;
+  auto& o = G.o;
+  for (int d = 16; d >= 1; d >>= 1)
+    for (int t : *pending) o << "gt" << t << "+=__shfl_xor_sync(0xffffffffu,gt" << t << "," << d << ");";
+  o << "if((threadIdx.x&31u)==0u){double* gw=ga+(threadIdx.x>>5)*" << nt << ";";
+  for (int t : *pending) o << "gw[" << t << "]+=(double)gt" << t << ";";
+  o << "}\n";
+  pending->clear();
 }
 
 const char* kPrelude = R"(
@@ -870,9 +886,12 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       int A = -1;
       for (int j = 0; j < pd.r; ++j)
         if (ph.rbit[j] == 0) A = j;
+      std::vector<int> pending;  // the phase's term accumulators not yet reduced
       auto term = [&](int gi) {
         const int k = ph.gate0 + gi;
-        if (grad && prog.grad_gen[k]) gen_term(G, gis[k], prog.grad_gen[k], prog.grad_term[k] - t0, A);
+        if (!grad || !prog.grad_gen[k]) return;
+        gen_term(G, gis[k], prog.grad_gen[k], prog.grad_term[k] - t0, A, &pending);
+        if ((int)pending.size() >= kTermBatch) gen_term_flush(G, &pending, std::max(1, nt));
       };
       for (int gi = 0; gi < ph.ngate; ++gi)
         if (fixed_diag(gis[ph.gate0 + gi])) {
@@ -905,6 +924,7 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         d.var = "fa";
         G.scale(d);
       }
+      gen_term_flush(G, &pending, std::max(1, nt));
       // local bits left flipped by the phase's bit-flip frame
       G.o << "return 0u";
       for (int j = 0; j < pd.r; ++j)
@@ -932,13 +952,17 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
       // added to the program's term array once at the end
       if (cfg.blocks != 2 || !all_active_g || pd.nphase == 0)
         throw std::runtime_error("jit: gradient programs run single-buffered blocks with every thread active");
+      // one row of terms per warp (rows: max_threads / 32)
+      const int ntr = std::max(1, nt), rows = hdr->max_threads / 32;
+      if (hdr->max_threads % 32) throw std::runtime_error("jit: gradient programs need whole warps");
       G.o << "extern \"C\" __global__ void __launch_bounds__(" << hdr->max_threads << ",2) " << kname
           << "(const uint8_t* __restrict__ prog,float2* __restrict__ psi,unsigned* __restrict__ err,"
           << "double* __restrict__ gterm,const __grid_constant__ KP" << p << " kp){__shared__ double ga_["
-          << std::max(1, nt) << "];for(int j=threadIdx.x;j<" << nt << ";j+=blockDim.x)ga_[j]=0.0;const X" << p
+          << rows * ntr << "];for(int j=threadIdx.x;j<" << rows * ntr << ";j+=blockDim.x)ga_[j]=0.0;const X" << p
           << " ex{&kp,ga_};qsb::pass_body_direct<float," << pd.r << ",X" << p << "," << pd.nphase << ">(ex,prog,psi,"
-          << p << ");__syncthreads();for(int j=threadIdx.x;j<" << nt << ";j+=blockDim.x){const double v=ga_[j];"
-          << "if(v!=0.0)atomicAdd(gterm+" << t0 << "+j,v);}}\n";
+          << p << ");__syncthreads();for(int j=threadIdx.x;j<" << nt << ";j+=blockDim.x){double v=0.0;"
+          << "for(int w=0;w<" << rows << ";++w)v+=ga_[w*" << ntr << "+j];if(v!=0.0)atomicAdd(gterm+" << t0
+          << "+j,v);}}\n";
       continue;
     }
     G.o << "extern \"C\" __global__ void __launch_bounds__("

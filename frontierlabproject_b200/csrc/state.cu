@@ -1029,7 +1029,7 @@ bool same_grad_structure(const std::vector<GradOp>& a, const std::vector<GradOp>
 
 PlanConfig grad_plan_cfg(int n, const qs_config* c) {
   PlanConfig p;
-  p.r = 5;
+  p.r = c && (c->jit_lr == 5 || c->jit_lr == 6) ? c->jit_lr : 5;
   p.m = c && c->m > 0 ? c->m : 13;
   p.k = c && c->k > 0 ? c->k : 3;
   p.hill_iters = c ? c->hill_iters : 16;
@@ -1229,6 +1229,7 @@ int qs_grad_create(int num_qubits, const qs_adj_op* ops, int nops, int nparams, 
       if (cfg->m > 0) s->cfg.m = std::min(cfg->m, 13);
       if (cfg->k > 0) s->cfg.k = cfg->k;
       s->cfg.hill_iters = cfg->hill_iters;
+      if (cfg->jit_lr == 5 || cfg->jit_lr == 6) s->jit_lr = cfg->jit_lr;
     }
     CK(dev_malloc(&g->phi, (sizeof(float) * 2) << (num_qubits + 1)));
     *out = g.release();

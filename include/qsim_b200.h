@@ -218,7 +218,8 @@ QS_API int qs_adjoint_sweep(qs_state* psi, qs_state* lam, const qs_adj_op* ops, 
  * (both states uncomputed by the same U_k^dagger), whose kernels add Im <lam|G|psi> before
  * each rotation into per-gate FP64 terms.  Plans and kernels follow the circuit's structure
  * (gate kinds, qubits, generators, slots): new parameter values reuse them.  10 <= n <= 33.
- * cfg (optional): m, k and hill_iters of the plans (other fields ignored). */
+ * cfg (optional): m, k and hill_iters of the plans and jit_lr (5 or 6 register bits per
+ * thread; the reverse program holds the lam bit in one of them); other fields ignored. */
 typedef struct qs_grad qs_grad;
 QS_API int qs_grad_create(int num_qubits, const qs_adj_op* ops, int nops, int nparams, const qs_config* cfg,
                           qs_grad** out);
