@@ -34,6 +34,14 @@ __device__ __forceinline__ uint64_t gtime() {
   return t;
 }
 
+// every thread of the block calls it (full warps); FP32 warp sum of per-thread FP32 terms,
+// added in FP64
+__device__ __forceinline__ void warp_addf(float v, double* dst) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0f) atomicAdd(dst, (double)v);
+}
+
 // every thread of the block calls it (full warps)
 __device__ __forceinline__ void warp_add(double v, double* dst) {
 #pragma unroll
@@ -174,13 +182,15 @@ __device__ void apply_gate(const BatchGate& gref, float2* A, float2* L, int m, u
           }
         }
       } else if (j0 >= 0 || j1 >= 0) {
-        // block-diagonal in the fixed qubit: the 2x2 block of its value on the staged one
+        // block-diagonal in the fixed qubit: the 2x2 block of its value on the staged one (entries
+        // read from the gate at a run-time index, not from the register copy)
+        auto G = [&](int r, int c) { return kRev ? cconj(gref.u[4 * c + r]) : gref.u[4 * r + c]; };
         if (j1 >= 0) {
           const int f = (int)((gb >> q0) & 1ull);
-          pairs2<kRev>(M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), 0, A, L, m, j1, acc);
+          pairs2<kRev>(G(f, f), G(f, f + 2), G(f + 2, f), G(f + 2, f + 2), 0, A, L, m, j1, acc);
         } else {
           const int f = (int)((gb >> q1) & 1ull);
-          pairs2<kRev>(M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f), M(2 * f + 1, 2 * f + 1), 0, A, L,
+          pairs2<kRev>(G(2 * f, 2 * f), G(2 * f, 2 * f + 1), G(2 * f + 1, 2 * f), G(2 * f + 1, 2 * f + 1), 0, A, L,
                        m, j0, acc);
         }
       }
@@ -246,6 +256,48 @@ __device__ __forceinline__ void pairs_reg(float2 m0, float2 m1, float2 m2, float
   }
 }
 
+// Real 2x2 (m0 m1; m2 m3) on register bit J: two multiply-adds per output component
+template <int J, bool kRev, int GEN>
+__device__ __forceinline__ void pairs_reg_real(float m0, float m1, float m2, float m3, float2 (&a)[kRegs],
+                                               float2 (&l)[kRegs], float& acc) {
+#pragma unroll
+  for (int i = 0; i < kRegs; ++i) {
+    if (i & (1 << J)) continue;
+    const int i1 = i | (1 << J);
+    const float2 p0 = a[i], p1 = a[i1];
+    a[i] = make_float2(m0 * p0.x + m1 * p1.x, m0 * p0.y + m1 * p1.y);
+    a[i1] = make_float2(m2 * p0.x + m3 * p1.x, m2 * p0.y + m3 * p1.y);
+    if (kRev) {
+      const float2 l0 = l[i], l1 = l[i1];
+      if (GEN == 1) acc += im_cvf(l0, p1) + im_cvf(l1, p0);
+      if (GEN == 2) acc += im_cvf(l0, make_float2(p1.y, -p1.x)) + im_cvf(l1, make_float2(-p0.y, p0.x));
+      if (GEN == 3) acc += im_cvf(l0, p0) - im_cvf(l1, p1);
+      l[i] = make_float2(m0 * l0.x + m1 * l1.x, m0 * l0.y + m1 * l1.y);
+      l[i1] = make_float2(m2 * l0.x + m3 * l1.x, m2 * l0.y + m3 * l1.y);
+    }
+  }
+}
+
+template <int J, bool kRev>
+__device__ __forceinline__ void pairs_reg_real_g(int gen, float m0, float m1, float m2, float m3, float2 (&a)[kRegs],
+                                                 float2 (&l)[kRegs], float& acc) {
+  if (!kRev || gen == 0) pairs_reg_real<J, kRev, 0>(m0, m1, m2, m3, a, l, acc);
+  else if (gen == 1) pairs_reg_real<J, kRev, 1>(m0, m1, m2, m3, a, l, acc);
+  else if (gen == 2) pairs_reg_real<J, kRev, 2>(m0, m1, m2, m3, a, l, acc);
+  else pairs_reg_real<J, kRev, 3>(m0, m1, m2, m3, a, l, acc);
+}
+
+template <bool kRev>
+__device__ __forceinline__ void pairs_reg_real_j(int j, int gen, float m0, float m1, float m2, float m3,
+                                                 float2 (&a)[kRegs], float2 (&l)[kRegs], float& acc) {
+  switch (j) {
+    case 0: pairs_reg_real_g<0, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    case 1: pairs_reg_real_g<1, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    case 2: pairs_reg_real_g<2, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+    default: pairs_reg_real_g<3, kRev>(gen, m0, m1, m2, m3, a, l, acc); break;
+  }
+}
+
 template <int J, bool kRev>
 __device__ __forceinline__ void pairs_reg_g(int gen, float2 m0, float2 m1, float2 m2, float2 m3, float2 (&a)[kRegs],
                                             float2 (&l)[kRegs], float& acc) {
@@ -253,6 +305,68 @@ __device__ __forceinline__ void pairs_reg_g(int gen, float2 m0, float2 m1, float
   else if (gen == 1) pairs_reg<J, kRev, 1>(m0, m1, m2, m3, a, l, acc);
   else if (gen == 2) pairs_reg<J, kRev, 2>(m0, m1, m2, m3, a, l, acc);
   else pairs_reg<J, kRev, 3>(m0, m1, m2, m3, a, l, acc);
+}
+
+// Diagonal (e0 where register bit J is 0, e1 where it is 1); kZ: acc += Im <L|Z_J|A> first.
+// The entry of each register is a compile-time choice (no per-amplitude selects).
+template <int J, bool kRev, bool kZ>
+__device__ __forceinline__ void diag_reg1(float2 e0, float2 e1, float2 (&a)[kRegs], float2 (&l)[kRegs], float& acc) {
+#pragma unroll
+  for (int i = 0; i < kRegs; ++i) {
+    const bool one = (i >> J) & 1;
+    const float2 p = a[i];
+    a[i] = cmul(one ? e1 : e0, p);
+    if (kRev) {
+      if (kZ) acc += one ? -im_cvf(l[i], p) : im_cvf(l[i], p);
+      l[i] = cmul(one ? e1 : e0, l[i]);
+    }
+  }
+}
+
+template <bool kRev, bool kZ>
+__device__ __forceinline__ void diag_reg1_j(int j, float2 e0, float2 e1, float2 (&a)[kRegs], float2 (&l)[kRegs],
+                                            float& acc) {
+  switch (j) {
+    case 0: diag_reg1<0, kRev, kZ>(e0, e1, a, l, acc); break;
+    case 1: diag_reg1<1, kRev, kZ>(e0, e1, a, l, acc); break;
+    case 2: diag_reg1<2, kRev, kZ>(e0, e1, a, l, acc); break;
+    default: diag_reg1<3, kRev, kZ>(e0, e1, a, l, acc); break;
+  }
+}
+
+// Diagonal d[b_J0 + 2 b_J1] on two register bits
+template <int J0, int J1, bool kRev>
+__device__ __forceinline__ void diag_reg2(float2 d0, float2 d1, float2 d2, float2 d3, float2 (&a)[kRegs],
+                                          float2 (&l)[kRegs]) {
+#pragma unroll
+  for (int i = 0; i < kRegs; ++i) {
+    const int v = ((i >> J0) & 1) | (((i >> J1) & 1) << 1);
+    const float2 dd = v == 0 ? d0 : v == 1 ? d1 : v == 2 ? d2 : d3;
+    a[i] = cmul(dd, a[i]);
+    if (kRev) l[i] = cmul(dd, l[i]);
+  }
+}
+
+template <int J0, bool kRev>
+__device__ __forceinline__ void diag_reg2_j1(int j1, float2 d0, float2 d1, float2 d2, float2 d3, float2 (&a)[kRegs],
+                                             float2 (&l)[kRegs]) {
+  switch (j1) {
+    case 0: if constexpr (J0 != 0) diag_reg2<J0, 0, kRev>(d0, d1, d2, d3, a, l); break;
+    case 1: if constexpr (J0 != 1) diag_reg2<J0, 1, kRev>(d0, d1, d2, d3, a, l); break;
+    case 2: if constexpr (J0 != 2) diag_reg2<J0, 2, kRev>(d0, d1, d2, d3, a, l); break;
+    default: if constexpr (J0 != 3) diag_reg2<J0, 3, kRev>(d0, d1, d2, d3, a, l); break;
+  }
+}
+
+template <bool kRev>
+__device__ __forceinline__ void diag_reg2_j(int j0, int j1, float2 d0, float2 d1, float2 d2, float2 d3,
+                                            float2 (&a)[kRegs], float2 (&l)[kRegs]) {
+  switch (j0) {
+    case 0: diag_reg2_j1<0, kRev>(j1, d0, d1, d2, d3, a, l); break;
+    case 1: diag_reg2_j1<1, kRev>(j1, d0, d1, d2, d3, a, l); break;
+    case 2: diag_reg2_j1<2, kRev>(j1, d0, d1, d2, d3, a, l); break;
+    default: diag_reg2_j1<3, kRev>(j1, d0, d1, d2, d3, a, l); break;
+  }
 }
 
 template <bool kRev>
@@ -279,30 +393,59 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
   };
   if (kind == BG_1Q) {
     const float2 u0 = gref.u[0], u1 = gref.u[1], u2 = gref.u[2], u3 = gref.u[3];
-    if (!kRev) pairs_reg_j<false>(reg[q0], 0, u0, u1, u2, u3, a, l, acc);
-    else pairs_reg_j<true>(reg[q0], gen, cconj(u0), cconj(u2), cconj(u1), cconj(u3), a, l, acc);
-  } else if (kind == BG_DIAG1 || kind == BG_DIAG2) {
-    const bool two = kind == BG_DIAG2;
-    float2 d[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const float2 v = (two || e < 2) ? gref.u[two ? e : (e & 1)] : make_float2(0.f, 0.f);
-      d[e] = kRev ? cconj(v) : v;
+    if (u0.y == 0.f && u1.y == 0.f && u2.y == 0.f && u3.y == 0.f) {  // real (RY, H): gate-uniform branch
+      if (!kRev) pairs_reg_real_j<false>(reg[q0], 0, u0.x, u1.x, u2.x, u3.x, a, l, acc);
+      else pairs_reg_real_j<true>(reg[q0], gen, u0.x, u2.x, u1.x, u3.x, a, l, acc);
+    } else if (!kRev) {
+      pairs_reg_j<false>(reg[q0], 0, u0, u1, u2, u3, a, l, acc);
+    } else {
+      pairs_reg_j<true>(reg[q0], gen, cconj(u0), cconj(u2), cconj(u1), cconj(u3), a, l, acc);
     }
-    if (!two) { d[2] = d[0]; d[3] = d[1]; }
-    const int j0 = reg[q0], f0 = j0 >= 0 ? 0 : fixedbit(q0);
-    const int j1 = two ? reg[q1] : -1, f1 = (two && j1 < 0) ? fixedbit(q1) : 0;
-    const bool z = kRev && gen == 3;
+  } else if (kind == BG_DIAG1 || kind == BG_DIAG2) {
+    // bits held in registers select the entry per register at compile time; fixed bits select
+    // once per thread
+    const bool two = kind == BG_DIAG2;
+    auto ent = [&](int e) { const float2 v = gref.u[e]; return kRev ? cconj(v) : v; };
+    const int j0 = reg[q0];
+    if (!two) {
+      const float2 d0 = ent(0), d1 = ent(1);
+      const bool z = kRev && gen == 3;
+      if (j0 >= 0) {
+        if (z) diag_reg1_j<kRev, true>(j0, d0, d1, a, l, acc);
+        else diag_reg1_j<kRev, false>(j0, d0, d1, a, l, acc);
+      } else {
+        const int f0 = fixedbit(q0);
+        const float2 dd = f0 ? d1 : d0;
 #pragma unroll
-    for (int i = 0; i < kRegs; ++i) {
-      const int b0 = j0 >= 0 ? ((i >> j0) & 1) : f0;
-      const int b1 = j1 >= 0 ? ((i >> j1) & 1) : f1;
-      const float2 dd = b1 ? (b0 ? d[3] : d[2]) : (b0 ? d[1] : d[0]);
-      const float2 p = a[i];
-      a[i] = cmul(dd, p);
-      if (kRev) {
-        if (z) acc += b0 ? -im_cvf(l[i], p) : im_cvf(l[i], p);
-        l[i] = cmul(dd, l[i]);
+        for (int i = 0; i < kRegs; ++i) {
+          const float2 p = a[i];
+          a[i] = cmul(dd, p);
+          if (kRev) {
+            if (z) acc += im_cvf(l[i], p);
+            l[i] = cmul(dd, l[i]);
+          }
+        }
+        if (z && f0) acc = -acc;
+      }
+    } else {
+      const float2 d0 = ent(0), d1 = ent(1), d2 = ent(2), d3 = ent(3);
+      const int j1 = reg[q1];
+      if (j0 >= 0 && j1 >= 0) {
+        diag_reg2_j<kRev>(j0, j1, d0, d1, d2, d3, a, l);
+      } else if (j0 >= 0) {
+        const int f1 = fixedbit(q1);
+        diag_reg1_j<kRev, false>(j0, f1 ? d2 : d0, f1 ? d3 : d1, a, l, acc);
+      } else if (j1 >= 0) {
+        const int f0 = fixedbit(q0);
+        diag_reg1_j<kRev, false>(j1, f0 ? d1 : d0, f0 ? d3 : d2, a, l, acc);
+      } else {
+        const int v = fixedbit(q0) + 2 * fixedbit(q1);
+        const float2 dd = v == 0 ? d0 : v == 1 ? d1 : v == 2 ? d2 : d3;
+#pragma unroll
+        for (int i = 0; i < kRegs; ++i) {
+          a[i] = cmul(dd, a[i]);
+          if (kRev) l[i] = cmul(dd, l[i]);
+        }
       }
     }
   } else if (kind == BG_2Q) {
@@ -317,7 +460,7 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
                         M(2 * f + 1, 2 * f + 1), a, l, acc);
     }
   }
-  if (kRev && gen) warp_add((double)acc, gout + gref.grad);
+  if (kRev && gen) warp_addf(acc, gout + gref.grad);
 }
 
 // All register phases of a pass on the staged group (kRev: phases and gates in reverse).
