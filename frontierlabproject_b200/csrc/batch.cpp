@@ -140,18 +140,31 @@ BatchGate encode_gate(const IGate& ig) {
   g.gen = (uint8_t)ig.gen;
   g.grad = ig.gen ? ig.grad : 0;
   auto f2 = [](cplx z) { return float2{(float)z.real(), (float)z.imag()}; };
+  // A diagonal unitary is stored divided by its first entry (a phase): the states then carry a
+  // phase common to psi and lam, which cancels in the energy <psi|H psi> and in every term
+  // Im <lam|G|psi>; the kernel skips the multiplies by the exact 1 this leaves.
+  auto unit_first = [](cplx* d, int k) {
+    const cplx d0 = d[0];
+    if (std::abs(std::abs(d0) - 1.0) > 1e-9) return;
+    for (int e = 0; e < k; ++e) d[e] /= d0;
+    d[0] = cplx(1.0, 0.0);
+  };
   if (ig.op.arity == 1) {
     if (diag1(ig)) {
       g.kind = BG_DIAG1;
-      g.u[0] = f2(ig.op.U[0]);
-      g.u[1] = f2(ig.op.U[3]);
+      cplx d[2] = {ig.op.U[0], ig.op.U[3]};
+      unit_first(d, 2);
+      g.u[0] = f2(d[0]);
+      g.u[1] = f2(d[1]);
     } else {
       g.kind = BG_1Q;
       for (int e = 0; e < 4; ++e) g.u[e] = f2(ig.op.U[e]);
     }
   } else if (c.kind == GK_2Q_DIAG) {
     g.kind = BG_DIAG2;
-    for (int e = 0; e < 4; ++e) g.u[e] = f2(ig.op.U[5 * e]);
+    cplx d[4] = {ig.op.U[0], ig.op.U[5], ig.op.U[10], ig.op.U[15]};
+    unit_first(d, 4);
+    for (int e = 0; e < 4; ++e) g.u[e] = f2(d[e]);
   } else {
     g.kind = BG_2Q;
     for (int e = 0; e < 16; ++e) g.u[e] = f2(ig.op.U[e]);

@@ -308,65 +308,87 @@ __device__ __forceinline__ void pairs_reg_g(int gen, float2 m0, float2 m1, float
 }
 
 // Diagonal (e0 where register bit J is 0, e1 where it is 1); kZ: acc += Im <L|Z_J|A> first.
-// The entry of each register is a compile-time choice (no per-amplitude selects).
-template <int J, bool kRev, bool kZ>
+// The entry of each register is a compile-time choice (no per-amplitude selects); kUnit0: e0
+// is exactly 1 (diagonal gates are stored divided by their first entry), its registers skip.
+template <int J, bool kRev, bool kZ, bool kUnit0>
 __device__ __forceinline__ void diag_reg1(float2 e0, float2 e1, float2 (&a)[kRegs], float2 (&l)[kRegs], float& acc) {
 #pragma unroll
   for (int i = 0; i < kRegs; ++i) {
     const bool one = (i >> J) & 1;
     const float2 p = a[i];
+    if (kRev && kZ) acc += one ? -im_cvf(l[i], p) : im_cvf(l[i], p);
+    if (kUnit0 && !one) continue;
     a[i] = cmul(one ? e1 : e0, p);
-    if (kRev) {
-      if (kZ) acc += one ? -im_cvf(l[i], p) : im_cvf(l[i], p);
-      l[i] = cmul(one ? e1 : e0, l[i]);
-    }
+    if (kRev) l[i] = cmul(one ? e1 : e0, l[i]);
   }
 }
 
 template <bool kRev, bool kZ>
 __device__ __forceinline__ void diag_reg1_j(int j, float2 e0, float2 e1, float2 (&a)[kRegs], float2 (&l)[kRegs],
                                             float& acc) {
-  switch (j) {
-    case 0: diag_reg1<0, kRev, kZ>(e0, e1, a, l, acc); break;
-    case 1: diag_reg1<1, kRev, kZ>(e0, e1, a, l, acc); break;
-    case 2: diag_reg1<2, kRev, kZ>(e0, e1, a, l, acc); break;
-    default: diag_reg1<3, kRev, kZ>(e0, e1, a, l, acc); break;
+  const bool u0 = e0.x == 1.f && e0.y == 0.f;
+  if (!kZ && u0 && e1.x == 1.f && e1.y == 0.f) return;  // identity here (a controlled phase off)
+  if (u0) {
+    switch (j) {
+      case 0: diag_reg1<0, kRev, kZ, true>(e0, e1, a, l, acc); break;
+      case 1: diag_reg1<1, kRev, kZ, true>(e0, e1, a, l, acc); break;
+      case 2: diag_reg1<2, kRev, kZ, true>(e0, e1, a, l, acc); break;
+      default: diag_reg1<3, kRev, kZ, true>(e0, e1, a, l, acc); break;
+    }
+  } else {
+    switch (j) {
+      case 0: diag_reg1<0, kRev, kZ, false>(e0, e1, a, l, acc); break;
+      case 1: diag_reg1<1, kRev, kZ, false>(e0, e1, a, l, acc); break;
+      case 2: diag_reg1<2, kRev, kZ, false>(e0, e1, a, l, acc); break;
+      default: diag_reg1<3, kRev, kZ, false>(e0, e1, a, l, acc); break;
+    }
   }
 }
 
-// Diagonal d[b_J0 + 2 b_J1] on two register bits
-template <int J0, int J1, bool kRev>
+// Diagonal d[b_J0 + 2 b_J1] on two register bits; kUnit: mask of entries that are exactly 1
+// (1: d0; 7: d0, d1 and d2, a controlled phase such as CZ), whose registers skip
+template <int J0, int J1, bool kRev, int kUnit>
 __device__ __forceinline__ void diag_reg2(float2 d0, float2 d1, float2 d2, float2 d3, float2 (&a)[kRegs],
                                           float2 (&l)[kRegs]) {
 #pragma unroll
   for (int i = 0; i < kRegs; ++i) {
     const int v = ((i >> J0) & 1) | (((i >> J1) & 1) << 1);
+    if ((kUnit >> v) & 1) continue;
     const float2 dd = v == 0 ? d0 : v == 1 ? d1 : v == 2 ? d2 : d3;
     a[i] = cmul(dd, a[i]);
     if (kRev) l[i] = cmul(dd, l[i]);
   }
 }
 
-template <int J0, bool kRev>
+template <int J0, bool kRev, int kUnit>
 __device__ __forceinline__ void diag_reg2_j1(int j1, float2 d0, float2 d1, float2 d2, float2 d3, float2 (&a)[kRegs],
                                              float2 (&l)[kRegs]) {
   switch (j1) {
-    case 0: if constexpr (J0 != 0) diag_reg2<J0, 0, kRev>(d0, d1, d2, d3, a, l); break;
-    case 1: if constexpr (J0 != 1) diag_reg2<J0, 1, kRev>(d0, d1, d2, d3, a, l); break;
-    case 2: if constexpr (J0 != 2) diag_reg2<J0, 2, kRev>(d0, d1, d2, d3, a, l); break;
-    default: if constexpr (J0 != 3) diag_reg2<J0, 3, kRev>(d0, d1, d2, d3, a, l); break;
+    case 0: if constexpr (J0 != 0) diag_reg2<J0, 0, kRev, kUnit>(d0, d1, d2, d3, a, l); break;
+    case 1: if constexpr (J0 != 1) diag_reg2<J0, 1, kRev, kUnit>(d0, d1, d2, d3, a, l); break;
+    case 2: if constexpr (J0 != 2) diag_reg2<J0, 2, kRev, kUnit>(d0, d1, d2, d3, a, l); break;
+    default: if constexpr (J0 != 3) diag_reg2<J0, 3, kRev, kUnit>(d0, d1, d2, d3, a, l); break;
+  }
+}
+
+template <bool kRev, int kUnit>
+__device__ __forceinline__ void diag_reg2_u(int j0, int j1, float2 d0, float2 d1, float2 d2, float2 d3,
+                                            float2 (&a)[kRegs], float2 (&l)[kRegs]) {
+  switch (j0) {
+    case 0: diag_reg2_j1<0, kRev, kUnit>(j1, d0, d1, d2, d3, a, l); break;
+    case 1: diag_reg2_j1<1, kRev, kUnit>(j1, d0, d1, d2, d3, a, l); break;
+    case 2: diag_reg2_j1<2, kRev, kUnit>(j1, d0, d1, d2, d3, a, l); break;
+    default: diag_reg2_j1<3, kRev, kUnit>(j1, d0, d1, d2, d3, a, l); break;
   }
 }
 
 template <bool kRev>
 __device__ __forceinline__ void diag_reg2_j(int j0, int j1, float2 d0, float2 d1, float2 d2, float2 d3,
                                             float2 (&a)[kRegs], float2 (&l)[kRegs]) {
-  switch (j0) {
-    case 0: diag_reg2_j1<0, kRev>(j1, d0, d1, d2, d3, a, l); break;
-    case 1: diag_reg2_j1<1, kRev>(j1, d0, d1, d2, d3, a, l); break;
-    case 2: diag_reg2_j1<2, kRev>(j1, d0, d1, d2, d3, a, l); break;
-    default: diag_reg2_j1<3, kRev>(j1, d0, d1, d2, d3, a, l); break;
-  }
+  auto is1 = [](float2 v) { return v.x == 1.f && v.y == 0.f; };
+  if (!is1(d0)) diag_reg2_u<kRev, 0>(j0, j1, d0, d1, d2, d3, a, l);
+  else if (is1(d1) && is1(d2)) { if (!is1(d3)) diag_reg2_u<kRev, 7>(j0, j1, d0, d1, d2, d3, a, l); }
+  else diag_reg2_u<kRev, 1>(j0, j1, d0, d1, d2, d3, a, l);
 }
 
 template <bool kRev>
@@ -416,13 +438,14 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
       } else {
         const int f0 = fixedbit(q0);
         const float2 dd = f0 ? d1 : d0;
+        const bool unit = dd.x == 1.f && dd.y == 0.f;
 #pragma unroll
         for (int i = 0; i < kRegs; ++i) {
           const float2 p = a[i];
-          a[i] = cmul(dd, p);
-          if (kRev) {
-            if (z) acc += im_cvf(l[i], p);
-            l[i] = cmul(dd, l[i]);
+          if (z) acc += im_cvf(l[i], p);
+          if (!unit) {
+            a[i] = cmul(dd, p);
+            if (kRev) l[i] = cmul(dd, l[i]);
           }
         }
         if (z && f0) acc = -acc;
@@ -441,10 +464,12 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
       } else {
         const int v = fixedbit(q0) + 2 * fixedbit(q1);
         const float2 dd = v == 0 ? d0 : v == 1 ? d1 : v == 2 ? d2 : d3;
+        if (dd.x != 1.f || dd.y != 0.f) {
 #pragma unroll
-        for (int i = 0; i < kRegs; ++i) {
-          a[i] = cmul(dd, a[i]);
-          if (kRev) l[i] = cmul(dd, l[i]);
+          for (int i = 0; i < kRegs; ++i) {
+            a[i] = cmul(dd, a[i]);
+            if (kRev) l[i] = cmul(dd, l[i]);
+          }
         }
       }
     }
