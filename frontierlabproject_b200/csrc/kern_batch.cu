@@ -404,9 +404,20 @@ __device__ __forceinline__ void pairs_reg_j(int j, int gen, float2 m0, float2 m1
 
 // One gate of a register phase.  reg[q]: register bit of qubit q in this phase (-1: not in
 // registers); fixed bits come from the slot's local base index or the group base.
-template <bool kRev>
-__device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* reg, const int8_t* loc, uint32_t base,
-                                         uint64_t gb, float2 (&a)[kRegs], float2 (&l)[kRegs], double* gout) {
+// A gate of the current pass as the register phases read it, cached in shared memory when the
+// pass changes (shared-memory latency instead of L1 for the per-gate fields); two-qubit dense
+// matrices stay in global memory (gfull).
+struct GateLite {
+  uint8_t kind, q0, q1, gen;
+  int32_t grad;
+  float2 u[4];
+};
+constexpr int kGateCache = 192;
+
+template <bool kRev, typename GT>
+__device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull, const int8_t* reg, const int8_t* loc,
+                                         uint32_t base, uint64_t gb, float2 (&a)[kRegs], float2 (&l)[kRegs],
+                                         double* gout) {
   float acc = 0.0f;
   const int kind = gref.kind, q0 = gref.q0, q1 = gref.q1, gen = gref.gen;
   auto fixedbit = [&](int q) -> int {
@@ -475,7 +486,7 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
     }
   } else if (kind == BG_2Q) {
     // one operand in registers, the other fixed (block-diagonal in it): its 2x2 block
-    auto M = [&](int r, int c) { return kRev ? cconj(gref.u[4 * c + r]) : gref.u[4 * r + c]; };
+    auto M = [&](int r, int c) { return kRev ? cconj(gfull->u[4 * c + r]) : gfull->u[4 * r + c]; };
     if (reg[q1] >= 0) {
       const int f = fixedbit(q0);
       pairs_reg_j<kRev>(reg[q1], 0, M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), a, l, acc);
@@ -492,7 +503,8 @@ __device__ __forceinline__ void gate_reg(const BatchGate& gref, const int8_t* re
 // Shared-memory layout: local index l at A[swz64(l)] (L likewise).
 template <bool kRev>
 __device__ void run_phases(const BatchGate* gates, const BatchPhase* phs, int nph, float2* A, float2* L, int m,
-                           uint64_t gb, const int8_t* loc, int8_t* reg, double* gout) {
+                           uint64_t gb, const int8_t* loc, int8_t* reg, double* gout, const GateLite* sg, int gfirst,
+                           int ncached) {
   for (int hh = 0; hh < nph; ++hh) {
     const BatchPhase& ph = phs[kRev ? nph - 1 - hh : hh];
     const int nr = ph.nr;
@@ -528,8 +540,10 @@ __device__ void run_phases(const BatchGate* gates, const BatchPhase* phs, int np
         l[i] = (kRev && use) ? L[o] : make_float2(0.f, 0.f);
       }
       for (int k = 0; k < ph.ngate; ++k) {
-        const BatchGate& g = gates[kRev ? ph.gate0 + ph.ngate - 1 - k : ph.gate0 + k];
-        gate_reg<kRev>(g, reg, loc, base, gb, a, l, gout);
+        const int gi = kRev ? ph.gate0 + ph.ngate - 1 - k : ph.gate0 + k;
+        const int li = gi - gfirst;
+        if (li >= 0 && li < ncached) gate_reg<kRev>(sg[li], gates + gi, reg, loc, base, gb, a, l, gout);
+        else gate_reg<kRev>(gates[gi], gates + gi, reg, loc, base, gb, a, l, gout);
       }
 #pragma unroll
       for (int i = 0; i < kRegs; ++i) {
@@ -557,6 +571,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
   __shared__ uint64_t s_dep[128 + 64];     // local index -> global offset (bits 0-6 | 7-12)
   __shared__ uint64_t s_gdep[128 + 128];   // group index -> global offset (bits 0-6 | 7-13)
   __shared__ double s_coef[2 * kBatchMaxQubits];
+  __shared__ GateLite s_gate[kGateCache];  // the current pass's gates (register phases)
   __shared__ int s_item;
 
   const BatchHeader* hdr = reinterpret_cast<const BatchHeader*>(prog);
@@ -629,6 +644,15 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
         }
       }
       if ((int)t < 2 * n) s_coef[t] = coef[B.in.coef0 + t];
+      if (B.it.kind != BI_HAM && B.ps.nphase > 0)
+        for (int e = (int)t; e < B.ps.ngate && e < kGateCache; e += NT) {
+          const BatchGate& g = gates[B.ps.gate0 + e];
+          GateLite c;
+          c.kind = g.kind; c.q0 = g.q0; c.q1 = g.q1; c.gen = g.gen; c.grad = g.grad;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) c.u[k] = g.u[k];
+          s_gate[e] = c;
+        }
       __syncthreads();
       if (t == 0) B.key = key;
     }
@@ -643,11 +667,13 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
       __syncthreads();
       const BatchGate* gs = gates + B.ps.gate0;
       if (regs) {
-        run_phases<false>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, nullptr);
+        run_phases<false>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, nullptr, s_gate, B.ps.gate0,
+                          min(B.ps.ngate, kGateCache));
         const double e = hamiltonian<false, true>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
         warp_add(e, energy + it.inst);
         __syncthreads();
-        run_phases<true>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, gout);
+        run_phases<true>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, gout, s_gate, B.ps.gate0,
+                         min(B.ps.ngate, kGateCache));
       } else {
         for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, n, 0, B.loc, nullptr);
         const double e = hamiltonian<false>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
@@ -686,8 +712,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
         }
         __syncthreads();
         if (regs) {
-          if (!rev) run_phases<false>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, nullptr);
-          else run_phases<true>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, gout);
+          if (!rev) run_phases<false>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, nullptr, s_gate, B.ps.gate0,
+                                      min(B.ps.ngate, kGateCache));
+          else run_phases<true>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, gout, s_gate, B.ps.gate0,
+                                    min(B.ps.ngate, kGateCache));
         } else if (!rev) {
           for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, m, gb, B.loc, nullptr);
         } else {
