@@ -410,36 +410,40 @@ __device__ __forceinline__ void pairs_reg_j(int j, int gen, float2 m0, float2 m1
 struct GateLite {
   uint8_t kind, q0, q1, gen;
   int32_t grad;
+  int8_t r0, r1;   // register bit of q0 / q1 in the gate's phase, -1: not in registers
+  int8_t l0, l1;   // local bit of q0 / q1 in the pass, -1: a group bit
   float2 u[4];
 };
 constexpr int kGateCache = 192;
 
+// r0 / r1: register bits of the operands in this phase (-1: fixed), l0 / l1: their local bits
+// (-1: group bits)
 template <bool kRev, typename GT>
-__device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull, const int8_t* reg, const int8_t* loc,
+__device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull, int r0, int r1, int l0, int l1,
                                          uint32_t base, uint64_t gb, float2 (&a)[kRegs], float2 (&l)[kRegs],
                                          double* gout) {
   float acc = 0.0f;
   const int kind = gref.kind, q0 = gref.q0, q1 = gref.q1, gen = gref.gen;
   auto fixedbit = [&](int q) -> int {
-    const int L = loc[q];
+    const int L = q == q0 ? l0 : l1;
     return L >= 0 ? (int)((base >> L) & 1u) : (int)((gb >> q) & 1ull);
   };
   if (kind == BG_1Q) {
     const float2 u0 = gref.u[0], u1 = gref.u[1], u2 = gref.u[2], u3 = gref.u[3];
     if (u0.y == 0.f && u1.y == 0.f && u2.y == 0.f && u3.y == 0.f) {  // real (RY, H): gate-uniform branch
-      if (!kRev) pairs_reg_real_j<false>(reg[q0], 0, u0.x, u1.x, u2.x, u3.x, a, l, acc);
-      else pairs_reg_real_j<true>(reg[q0], gen, u0.x, u2.x, u1.x, u3.x, a, l, acc);
+      if (!kRev) pairs_reg_real_j<false>(r0, 0, u0.x, u1.x, u2.x, u3.x, a, l, acc);
+      else pairs_reg_real_j<true>(r0, gen, u0.x, u2.x, u1.x, u3.x, a, l, acc);
     } else if (!kRev) {
-      pairs_reg_j<false>(reg[q0], 0, u0, u1, u2, u3, a, l, acc);
+      pairs_reg_j<false>(r0, 0, u0, u1, u2, u3, a, l, acc);
     } else {
-      pairs_reg_j<true>(reg[q0], gen, cconj(u0), cconj(u2), cconj(u1), cconj(u3), a, l, acc);
+      pairs_reg_j<true>(r0, gen, cconj(u0), cconj(u2), cconj(u1), cconj(u3), a, l, acc);
     }
   } else if (kind == BG_DIAG1 || kind == BG_DIAG2) {
     // bits held in registers select the entry per register at compile time; fixed bits select
     // once per thread
     const bool two = kind == BG_DIAG2;
     auto ent = [&](int e) { const float2 v = gref.u[e]; return kRev ? cconj(v) : v; };
-    const int j0 = reg[q0];
+    const int j0 = r0;
     if (!two) {
       const float2 d0 = ent(0), d1 = ent(1);
       const bool z = kRev && gen == 3;
@@ -463,7 +467,7 @@ __device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull,
       }
     } else {
       const float2 d0 = ent(0), d1 = ent(1), d2 = ent(2), d3 = ent(3);
-      const int j1 = reg[q1];
+      const int j1 = r1;
       if (j0 >= 0 && j1 >= 0) {
         diag_reg2_j<kRev>(j0, j1, d0, d1, d2, d3, a, l);
       } else if (j0 >= 0) {
@@ -487,12 +491,12 @@ __device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull,
   } else if (kind == BG_2Q) {
     // one operand in registers, the other fixed (block-diagonal in it): its 2x2 block
     auto M = [&](int r, int c) { return kRev ? cconj(gfull->u[4 * c + r]) : gfull->u[4 * r + c]; };
-    if (reg[q1] >= 0) {
+    if (r1 >= 0) {
       const int f = fixedbit(q0);
-      pairs_reg_j<kRev>(reg[q1], 0, M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), a, l, acc);
+      pairs_reg_j<kRev>(r1, 0, M(f, f), M(f, f + 2), M(f + 2, f), M(f + 2, f + 2), a, l, acc);
     } else {
       const int f = fixedbit(q1);
-      pairs_reg_j<kRev>(reg[q0], 0, M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f),
+      pairs_reg_j<kRev>(r0, 0, M(2 * f, 2 * f), M(2 * f, 2 * f + 1), M(2 * f + 1, 2 * f),
                         M(2 * f + 1, 2 * f + 1), a, l, acc);
     }
   }
@@ -542,8 +546,15 @@ __device__ void run_phases(const BatchGate* gates, const BatchPhase* phs, int np
       for (int k = 0; k < ph.ngate; ++k) {
         const int gi = kRev ? ph.gate0 + ph.ngate - 1 - k : ph.gate0 + k;
         const int li = gi - gfirst;
-        if (li >= 0 && li < ncached) gate_reg<kRev>(sg[li], gates + gi, reg, loc, base, gb, a, l, gout);
-        else gate_reg<kRev>(gates[gi], gates + gi, reg, loc, base, gb, a, l, gout);
+        if (li >= 0 && li < ncached) {
+          const GateLite& c = sg[li];
+          gate_reg<kRev>(c, gates + gi, c.r0, c.r1, c.l0, c.l1, base, gb, a, l, gout);
+        } else {
+          const BatchGate& g = gates[gi];
+          const int two = g.kind == BG_DIAG2 || g.kind == BG_2Q;
+          gate_reg<kRev>(g, gates + gi, reg[g.q0], two ? reg[g.q1] : -1, loc[g.q0], two ? loc[g.q1] : -1, base, gb,
+                         a, l, gout);
+        }
       }
 #pragma unroll
       for (int i = 0; i < kRegs; ++i) {
@@ -649,6 +660,25 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
           const BatchGate& g = gates[B.ps.gate0 + e];
           GateLite c;
           c.kind = g.kind; c.q0 = g.q0; c.q1 = g.q1; c.gen = g.gen; c.grad = g.grad;
+          // the gate's phase and its operands' local / register bits (from the pass descriptors)
+          int h = 0;
+          while (h + 1 < B.ps.nphase && phases_g[B.ps.phase0 + h + 1].gate0 <= B.ps.gate0 + e) ++h;
+          const BatchPhase& gph = phases_g[B.ps.phase0 + h];
+          auto local_of = [&](int q) {
+            for (int j = 0; j < B.ps.m; ++j)
+              if (B.ps.sbit[j] == q) return j;
+            return -1;
+          };
+          auto reg_of = [&](int lb) {
+            for (int j = 0; j < gph.nr && lb >= 0; ++j)
+              if (gph.rbit[j] == lb) return j;
+            return -1;
+          };
+          const bool two = g.kind == BG_DIAG2 || g.kind == BG_2Q;
+          c.l0 = (int8_t)local_of(g.q0);
+          c.l1 = (int8_t)(two ? local_of(g.q1) : -1);
+          c.r0 = (int8_t)reg_of(c.l0);
+          c.r1 = (int8_t)(two ? reg_of(c.l1) : -1);
 #pragma unroll
           for (int k = 0; k < 4; ++k) c.u[k] = g.u[k];
           s_gate[e] = c;
