@@ -59,6 +59,12 @@ struct DeviceFault {
   std::string msg;
 };
 
+// a status returned by one of this library's own entry points, passed on unchanged
+struct Status {
+  int code;
+  std::string msg;
+};
+
 constexpr uint64_t kBarrierLimitNs = kDeviceWaitLimitNs;
 
 int reg_bits(int dtype) { return dtype == 0 ? 5 : 4; }
@@ -428,6 +434,8 @@ int guard(F&& f) {
     return fail(QS_ERR_INVALID, e.msg);
   } catch (const DeviceFault& e) {
     return fail(QS_ERR_DEVICE, e.msg);
+  } catch (const Status& e) {
+    return fail(e.code, e.msg);
   } catch (const CudaError& e) {
     return fail(QS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e.e));
   } catch (const std::exception& e) {
@@ -1222,7 +1230,7 @@ int qs_grad_create(int num_qubits, const qs_adj_op* ops, int nops, int nparams, 
     for (const PlannedPass& ps : g->rplan) g->rev_phases += (int)ps.phases.size();
     qs_state* s = nullptr;
     const int rc = qs_create(num_qubits, QS_C64, &s);
-    if (rc != 0) throw InvalidArg{std::string(qs_last_error())};
+    if (rc != 0) throw Status{rc, std::string(qs_last_error())};
     g->fwd = s;
     s->jit_mode = 1;
     if (cfg) {

@@ -118,3 +118,58 @@ def test_sampling_allocation_failure_is_clean():
             N.lib().qs_debug_fail_alloc(0)
     idx = sv.sample(1000, seed=3)
     assert idx.size == 1000 and np.all(np.diff(idx.astype(np.int64)) >= 0)
+
+
+def _grad_case(n=14, L=2, seed=3):
+    from frontierlabproject_b200.adjoint import AdjOps, ParamCircuit
+    pc = ParamCircuit.hea(n, L)
+    th = np.random.default_rng(seed).uniform(-np.pi, np.pi, pc.num_params)
+    a, b = C.hea_observable(n, seed)
+    tab = AdjOps(pc)  # owns the matrices the op table points to
+    return pc, th, a, b, tab, tab.update(th)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5])
+def test_gradient_handle_allocation_failure_frees_everything(k):
+    pc, th, a, b, tab, ops = _grad_case()
+    L = N.lib()
+    before = _free_bytes()
+    h = ctypes.c_void_p()
+    L.qs_debug_fail_alloc(k)
+    try:
+        rc = L.qs_grad_create(pc.num_qubits, ops.ctypes.data, len(ops), pc.num_params, None, ctypes.byref(h))
+    finally:
+        L.qs_debug_fail_alloc(0)
+    assert rc == N.QS_ERR_CUDA
+    assert b"out of memory" in L.qs_last_error()
+    assert not h.value
+    assert abs(_free_bytes() - before) < (16 << 20)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 6])
+def test_gradient_run_allocation_failure_then_runs(k):
+    # the k-th allocation of the first run (program buffers, staging, term array) fails: a clean
+    # error, and the same handle then gives the oracle's gradient
+    pc, th, a, b, tab, ops = _grad_case()
+    L = N.lib()
+    h = ctypes.c_void_p()
+    N.call("qs_grad_create", pc.num_qubits, ops.ctypes.data, len(ops), pc.num_params, None, ctypes.byref(h))
+    try:
+        E = ctypes.c_double()
+        G = np.zeros(pc.num_params)
+        L.qs_debug_fail_alloc(k)
+        try:
+            rc = L.qs_grad_run(h, ops.ctypes.data, len(ops), a.ctypes.data, b.ctypes.data, ctypes.byref(E),
+                               G.ctypes.data)
+        finally:
+            L.qs_debug_fail_alloc(0)
+        if rc != 0:
+            assert rc == N.QS_ERR_CUDA
+            assert b"out of memory" in L.qs_last_error()
+        N.call("qs_grad_run", h, ops.ctypes.data, len(ops), a.ctypes.data, b.ctypes.data, ctypes.byref(E),
+               G.ctypes.data)
+        E_ref, g_ref = O.adjoint_gradient(C.hea_ansatz(pc.num_qubits, 2, th), a, b)
+        assert abs(E.value - E_ref) <= 1e-5 * max(1.0, abs(E_ref))
+        assert np.linalg.norm(G - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+    finally:
+        L.qs_grad_destroy(h)
