@@ -508,18 +508,22 @@ __device__ __forceinline__ void gate_reg(const GT& gref, const BatchGate* gfull,
 template <bool kRev>
 __device__ void run_phases(const BatchGate* gates, const BatchPhase* phs, int nph, float2* A, float2* L, int m,
                            uint64_t gb, const int8_t* loc, int8_t* reg, double* gout, const GateLite* sg, int gfirst,
-                           int ncached) {
+                           int ncached, int npass_gates) {
+  // gates past the shared-memory cache look their register bits up in reg[] (rebuilt per phase)
+  const bool all_cached = ncached >= npass_gates;
   for (int hh = 0; hh < nph; ++hh) {
     const BatchPhase& ph = phs[kRev ? nph - 1 - hh : hh];
     const int nr = ph.nr;
-    if ((int)threadIdx.x < kBatchMaxQubits) {
-      const int q = threadIdx.x;
-      int r = -1;
-      for (int j = 0; j < nr; ++j)
-        if (loc[q] >= 0 && ph.rbit[j] == loc[q]) r = j;
-      reg[q] = (int8_t)r;
+    if (!all_cached) {
+      if ((int)threadIdx.x < kBatchMaxQubits) {
+        const int q = threadIdx.x;
+        int r = -1;
+        for (int j = 0; j < nr; ++j)
+          if (loc[q] >= 0 && ph.rbit[j] == loc[q]) r = j;
+        reg[q] = (int8_t)r;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     uint32_t RB[kBatchRegBits];
 #pragma unroll
     for (int j = 0; j < kBatchRegBits; ++j) RB[j] = j < nr ? swz64(1u << ph.rbit[j]) : 0u;
@@ -698,12 +702,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
       const BatchGate* gs = gates + B.ps.gate0;
       if (regs) {
         run_phases<false>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, nullptr, s_gate, B.ps.gate0,
-                          min(B.ps.ngate, kGateCache));
+                          min(B.ps.ngate, kGateCache), B.ps.ngate);
         const double e = hamiltonian<false, true>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
         warp_add(e, energy + it.inst);
         __syncthreads();
         run_phases<true>(gates, s_ph, B.ps.nphase, A, L, n, 0, B.loc, s_reg, gout, s_gate, B.ps.gate0,
-                         min(B.ps.ngate, kGateCache));
+                         min(B.ps.ngate, kGateCache), B.ps.ngate);
       } else {
         for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, n, 0, B.loc, nullptr);
         const double e = hamiltonian<false>(A, L, n, 0, (uint64_t)dim, s_coef, s_coef + n);
@@ -743,9 +747,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) batch_kernel(const uint8_t* __re
         __syncthreads();
         if (regs) {
           if (!rev) run_phases<false>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, nullptr, s_gate, B.ps.gate0,
-                                      min(B.ps.ngate, kGateCache));
+                                      min(B.ps.ngate, kGateCache), B.ps.ngate);
           else run_phases<true>(gates, s_ph, B.ps.nphase, A, L, m, gb, B.loc, s_reg, gout, s_gate, B.ps.gate0,
-                                    min(B.ps.ngate, kGateCache));
+                                    min(B.ps.ngate, kGateCache), B.ps.ngate);
         } else if (!rev) {
           for (int k = 0; k < B.ps.ngate; ++k) apply_gate<false>(gs[k], A, L, m, gb, B.loc, nullptr);
         } else {
