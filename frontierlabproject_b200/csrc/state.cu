@@ -1140,67 +1140,69 @@ struct qs_grad {
     // Phi = psi (+) H psi and the energy
     CK(launch_zz_x_stack(s->psi, phi, n, a, b, d_out, st));
     s->st.launches += 1;
-    // the reverse program: one launch per pass, captured as a graph (parameter values only
-    // update it)
-    JitConfig jc;
-    jc.blocks = 2;
-    jc.packed = false;
-    std::shared_ptr<JitKernels> jk = jit_get(gp.prog, jc);
-    s->st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
-    s->st.jit_modules += (unsigned long long)jk->chunks;
-    s->st.jit_disk_hits += (unsigned long long)jk->disk_hits;
-    jk->compile_seconds = 0.0;
-    jk->chunks = 0;
-    jk->disk_hits = 0;
-    const uint64_t key = jk->key ^ ((uint64_t)(uintptr_t)phi * 0x9E3779B97F4A7C15ull) ^
-                         ((uint64_t)(uintptr_t)d_prog << 1) ^ ((uint64_t)(uintptr_t)d_out << 3);
-    const uint64_t values = coef_values_hash(gp.prog);
-    const uint8_t* host_coef = gp.prog.bytes.data() + ((const ProgramHeader*)gp.prog.bytes.data())->off_coef;
-    auto capture = [&]() {
-      cudaGraph_t g = nullptr;
-      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      cudaError_t e = cudaSuccess;
-      for (int p = 0; p < gp.prog.npass && e == cudaSuccess; ++p)
-        e = jit_launch(*jk, p, d_prog, host_coef, phi, s->d_ctl + 2, gp.prog.threads, gp.prog.max_smem,
-                       device_sm_count(), st, d_out + 1);
-      cudaError_t e2 = cudaStreamEndCapture(st, &g);
-      if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
-      if (e2 != cudaSuccess) throw CudaError{e2};
-      return g;
-    };
-    bool updated = false;
-    if (graph.exec && graph.key == key && graph.values != values) {
-      cudaGraph_t g = capture();
-      cudaGraphExecUpdateResultInfo info;
-      const cudaError_t eu = cudaGraphExecUpdate(graph.exec, g, &info);
-      cudaGraphDestroy(g);
-      if (eu == cudaSuccess) {
-        graph.values = values;
-        updated = true;
-      } else {
-        cudaGetLastError();
-        CK(cudaGraphExecDestroy(graph.exec));
-        graph.exec = nullptr;
+    if (gp.prog.npass > 0) {  // (a circuit without gates has no reverse sweep: every term is zero)
+      // the reverse program: one launch per pass, captured as a graph (parameter values only
+      // update it)
+      JitConfig jc;
+      jc.blocks = 2;
+      jc.packed = false;
+      std::shared_ptr<JitKernels> jk = jit_get(gp.prog, jc);
+      s->st.jit_compile_ms += (unsigned long long)(jk->compile_seconds * 1e3 + 0.5);
+      s->st.jit_modules += (unsigned long long)jk->chunks;
+      s->st.jit_disk_hits += (unsigned long long)jk->disk_hits;
+      jk->compile_seconds = 0.0;
+      jk->chunks = 0;
+      jk->disk_hits = 0;
+      const uint64_t key = jk->key ^ ((uint64_t)(uintptr_t)phi * 0x9E3779B97F4A7C15ull) ^
+                           ((uint64_t)(uintptr_t)d_prog << 1) ^ ((uint64_t)(uintptr_t)d_out << 3);
+      const uint64_t values = coef_values_hash(gp.prog);
+      const uint8_t* host_coef = gp.prog.bytes.data() + ((const ProgramHeader*)gp.prog.bytes.data())->off_coef;
+      auto capture = [&]() {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int p = 0; p < gp.prog.npass && e == cudaSuccess; ++p)
+          e = jit_launch(*jk, p, d_prog, host_coef, phi, s->d_ctl + 2, gp.prog.threads, gp.prog.max_smem,
+                         device_sm_count(), st, d_out + 1);
+        cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); throw CudaError{e}; }
+        if (e2 != cudaSuccess) throw CudaError{e2};
+        return g;
+      };
+      bool updated = false;
+      if (graph.exec && graph.key == key && graph.values != values) {
+        cudaGraph_t g = capture();
+        cudaGraphExecUpdateResultInfo info;
+        const cudaError_t eu = cudaGraphExecUpdate(graph.exec, g, &info);
+        cudaGraphDestroy(g);
+        if (eu == cudaSuccess) {
+          graph.values = values;
+          updated = true;
+        } else {
+          cudaGetLastError();
+          CK(cudaGraphExecDestroy(graph.exec));
+          graph.exec = nullptr;
+        }
       }
+      if (!graph.exec || graph.key != key) {
+        if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
+        graph.kernels = jk;
+        cudaGraph_t g = capture();
+        cudaError_t e3 = cudaGraphInstantiate(&graph.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) throw CudaError{e3};
+        graph.key = key;
+        graph.values = values;
+        s->st.graph_builds += 1;
+      } else if (updated) {
+        s->st.graph_builds += 1;
+      } else {
+        s->st.graph_replays += 1;
+      }
+      CK(cudaGraphLaunch(graph.exec, st));
+      s->st.launches += 1;
+      s->st.sweeps += gp.prog.npass;
     }
-    if (!graph.exec || graph.key != key) {
-      if (graph.exec) { CK(cudaGraphExecDestroy(graph.exec)); graph.exec = nullptr; }
-      graph.kernels = jk;
-      cudaGraph_t g = capture();
-      cudaError_t e3 = cudaGraphInstantiate(&graph.exec, g, 0);
-      cudaGraphDestroy(g);
-      if (e3 != cudaSuccess) throw CudaError{e3};
-      graph.key = key;
-      graph.values = values;
-      s->st.graph_builds += 1;
-    } else if (updated) {
-      s->st.graph_builds += 1;
-    } else {
-      s->st.graph_replays += 1;
-    }
-    CK(cudaGraphLaunch(graph.exec, st));
-    s->st.launches += 1;
-    s->st.sweeps += gp.prog.npass;
     CK(cudaMemcpyAsync(h_out, d_out, outb, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     s->check_device_error();

@@ -93,3 +93,23 @@ def test_structure_change_is_rejected():
         assert np.linalg.norm(G - g_ref) <= 1e-5 * max(1.0, np.linalg.norm(g_ref))
     finally:
         N.lib().qs_grad_destroy(h)
+
+
+def test_circuit_without_gates_or_rotations():
+    # no gate at all (psi = |0...0>), and fixed gates only: the energy, with empty / zero gradients
+    from frontierlabproject_b200.adjoint import AdjointEngine, ParamCircuit, ParamGate
+    from frontierlabproject_b200.circuit import QuantumCircuit
+    n = 12
+    a, b = C.hea_observable(n, 2)
+    E, g = AdjointEngine(n, f32=True, method="jit").energy_and_grad(ParamCircuit(n, [], 0), [], a, b)
+    psi0 = np.zeros(1 << n, dtype=np.complex128)
+    psi0[0] = 1
+    assert abs(E - O.energy(psi0, a, b)) <= 1e-6 and g.size == 0
+    pc = ParamCircuit(n, [ParamGate("h", (q,)) for q in range(n)] + [ParamGate("cz", (0, 5))], 3)
+    qc = QuantumCircuit(n)
+    for q in range(n):
+        qc.h(q)
+    qc.cz(0, 5)
+    E, g = AdjointEngine(n, f32=True, method="jit").energy_and_grad(pc, [0.1, 0.2, 0.3], a, b)
+    assert abs(E - O.energy(O.simulate(qc), a, b)) <= 1e-5
+    assert np.all(g == 0.0) and g.size == 3
