@@ -219,6 +219,7 @@ Encoded encode_batch(const std::vector<Inst>& insts, const Cfg& cfg, PlanCache* 
     pc.r = std::min(kBatchRegBits, m);
     pc.k = std::min(3, m);
     pc.lookahead = 0;  // many small instances: planning time matters more than a sweep or two
+    pc.phase_lookahead = 0;
     uint64_t sig = 1469598103934665603ull ^ (uint64_t)m;
     for (const COp& c : cops) {
       const uint64_t w[3] = {c.need, c.touch, (uint64_t)c.kind};

@@ -351,8 +351,39 @@ std::vector<int> bits_of(uint64_t m) {
 
 }  // namespace
 
+// Every r-subset of the staged bits (containing `forced`): the register set of a phase that
+// executes the most gates (soft score of Scan).
+static uint64_t choose_phase_exhaustive(const Scan& sc, const std::vector<int>& rem, uint64_t Smask, uint64_t forced,
+                                        int r, std::vector<std::pair<size_t, uint64_t>>* top = nullptr) {
+  std::vector<int> free_bits;
+  for (int p : bits_of(Smask))
+    if (!(forced & bit(p))) free_bits.push_back(p);
+  const int need = r - __builtin_popcountll(forced);
+  const int nf = (int)free_bits.size();
+  uint64_t best = 0;
+  size_t best_v = 0;
+  bool have = false;
+  std::vector<int> idx(need);
+  for (int i = 0; i < need; ++i) idx[i] = i;
+  if (need <= 0 || need > nf) return forced;
+  for (;;) {
+    uint64_t R = forced;
+    for (int i : idx) R |= bit(free_bits[i]);
+    const size_t v = sc.count(rem, R);
+    if (!have || v > best_v) { best = R; best_v = v; have = true; }
+    if (top) top->push_back({v, R});
+    int i = need - 1;
+    while (i >= 0 && idx[i] == nf - need + i) --i;
+    if (i < 0) break;
+    ++idx[i];
+    for (int j = i + 1; j < need; ++j) idx[j] = idx[j - 1] + 1;
+  }
+  return best;
+}
+
 static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const std::vector<int>& pass_ops,
-                                             const std::vector<int>& sbits, int r, int iters, bool pair_bit) {
+                                             const std::vector<int>& sbits, int r, int iters, bool pair_bit,
+                                             int lookahead) {
   // Phases choose register bits among the staged physical bits; op need masks are
   // physical, so the phase set is a physical mask, converted to local bits at the end.
   uint64_t Smask = 0;
@@ -363,7 +394,39 @@ static std::vector<PlannedPhase> plan_phases(const std::vector<COp>& ops, const 
   std::vector<int> rem = pass_ops, taken, rest;
   while (!rem.empty()) {
     const uint64_t forced = (pair_bit && (Smask & 1ull)) ? 1ull : 0ull;
-    uint64_t R = choose_set(sc, rem, Smask, forced, rr, iters);
+    std::vector<std::pair<size_t, uint64_t>> top;
+    uint64_t R = 0;
+    if (lookahead <= 0) {
+      R = choose_set(sc, rem, Smask, forced, rr, iters);
+    } else {
+      // every register set is scored; among the `lookahead` best, the one after which greedy
+      // phases (best set each) finish the pass soonest
+      R = choose_phase_exhaustive(sc, rem, Smask, forced, rr, &top);
+      std::stable_sort(top.begin(), top.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+      if ((int)top.size() > lookahead) top.resize(lookahead);
+      int best_np = 1 << 30;
+      std::vector<int> r1, r2, tk;
+      auto drop = [&](const std::vector<int>& rr0, uint64_t X, std::vector<int>& out) {
+        sc.run(rr0, X, tk);
+        out.clear();
+        size_t t2 = 0;
+        for (int i : rr0) {
+          if (t2 < tk.size() && tk[t2] == i) { ++t2; continue; }
+          out.push_back(i);
+        }
+      };
+      for (const auto& c : top) {
+        drop(rem, c.second, r1);
+        int np = 1;
+        while (!r1.empty() && np < best_np) {
+          const uint64_t X = choose_phase_exhaustive(sc, r1, Smask, forced, rr);
+          drop(r1, X, r2);
+          r1.swap(r2);
+          ++np;
+        }
+        if (np < best_np) { best_np = np; R = c.second; }
+      }
+    }
     sc.run(rem, R, taken);
     if (taken.empty()) throw std::runtime_error("planner: phase made no progress");
     PlannedPhase ph;
@@ -438,7 +501,7 @@ std::vector<PlannedPass> plan_passes(const std::vector<COp>& ops, int n, const P
     PlannedPass ps;
     ps.sbits = bits_of(S);
     ps.ops = taken;
-    ps.phases = plan_phases(ops, taken, ps.sbits, cfg.r, cfg.hill_iters, cfg.pair_bit);
+    ps.phases = plan_phases(ops, taken, ps.sbits, cfg.r, cfg.hill_iters, cfg.pair_bit, cfg.phase_lookahead);
     out.push_back(std::move(ps));
     rest.clear();
     size_t t = 0;
