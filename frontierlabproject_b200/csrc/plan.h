@@ -47,7 +47,7 @@ struct PlanConfig {
                           // restarts of the staged-set search)
   bool pair_bit = false;  // physical bit 0 is a register bit of every phase (packed kernels)
   int lookahead = 2;      // staged-set choice: greedy passes looked ahead over the 4 best candidates
-  int phase_lookahead = 8;  // register sets: every set scored, and among this many best the one after
+  int phase_lookahead = 16;  // register sets: every set scored, and among this many best the one after
                             // which greedy phases finish the pass soonest (0: hill climbing only)
 };
 
