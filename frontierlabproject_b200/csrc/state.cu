@@ -1057,6 +1057,7 @@ struct qs_grad {
   uint8_t* d_prog = nullptr;
   size_t prog_cap = 0;
   uint8_t* h_prog = nullptr;       // pinned staging of the reverse program
+  cudaEvent_t copied = nullptr;    // the last copy out of h_prog has run
   size_t hprog_cap = 0;
   double* d_out = nullptr;         // energy, then the terms
   double* h_out = nullptr;         // pinned
@@ -1070,6 +1071,7 @@ struct qs_grad {
     if (phi) cudaFree(phi);
     if (d_prog) cudaFree(d_prog);
     if (h_prog) cudaFreeHost(h_prog);
+    if (copied) cudaEventDestroy(copied);
     if (d_out) cudaFree(d_out);
     if (h_out) cudaFreeHost(h_out);
     delete fwd;
@@ -1134,8 +1136,13 @@ struct qs_grad {
       prog_cap = hprog_cap = pb * 2;
       if (graph.exec) { cudaGraphExecDestroy(graph.exec); graph.exec = nullptr; }
     }
-    std::memcpy(h_prog, gp.prog.bytes.data(), pb);  // the previous run's copy has completed (run ends synchronised)
+    // the staging is rewritten only after its previous copy ran (a run that failed midway may
+    // have left one queued)
+    if (!copied) CK(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+    CK(cudaEventSynchronize(copied));
+    std::memcpy(h_prog, gp.prog.bytes.data(), pb);
     CK(cudaMemcpyAsync(d_prog, h_prog, pb, cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(copied, st));
     CK(cudaMemsetAsync(d_out, 0, outb, st));
     // Phi = psi (+) H psi and the energy
     CK(launch_zz_x_stack(s->psi, phi, n, a, b, d_out, st));
