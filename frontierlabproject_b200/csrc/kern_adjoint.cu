@@ -46,15 +46,32 @@ __device__ __forceinline__ void block_add(double v, double* acc) {
 // lam[2x] = psi[x] and lam[2x + 1] = (H psi)[x] (one 16-byte store).
 template <typename C, bool kStack = false>
 __global__ void zz_x_kernel(const C* __restrict__ psi, C* __restrict__ lam, int n, Coef cf, double* energy) {
+  // sum_i a_i Z_i Z_{i+1} = A - 2 sum_{i: y_i = 1} a_i with y = x XOR (x rotated right by one bit)
+  // (bit i of y: bits i and i+1 mod n differ); the partial sums of a over each 8-bit chunk of y
+  // are tabulated per block
+  __shared__ double s_tab[5][256];
+  __shared__ double s_atot;
+  for (int e = threadIdx.x; e < 5 * 256; e += blockDim.x) {
+    const int c = e >> 8, v = e & 255;
+    double t = 0.0;
+    for (int j = 0; j < 8; ++j)
+      if (((v >> j) & 1) && 8 * c + j < n) t += cf.a[8 * c + j];
+    s_tab[c][v] = t;
+  }
+  if (threadIdx.x == 0) {
+    double A = 0.0;
+    for (int i = 0; i < n; ++i) A += cf.a[i];
+    s_atot = A;
+  }
+  __syncthreads();
   const uint64_t dim = 1ull << n;
+  const int nchunk = (n + 7) / 8;
   double e = 0.0;
   for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
-    double d = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const int j = (i + 1) % n;
-      const int zz = (((x >> i) ^ (x >> j)) & 1ull) ? -1 : 1;
-      d += cf.a[i] * zz;
-    }
+    const uint64_t y = x ^ (((x >> 1) | ((x & 1ull) << (n - 1))) & (dim - 1));
+    double ssum = 0.0;
+    for (int c = 0; c < nchunk; ++c) ssum += s_tab[c][(y >> (8 * c)) & 255u];
+    const double d = s_atot - 2.0 * ssum;
     const C p = psi[x];
     double re = d * p.x, im = d * p.y;
     for (int i = 0; i < n; ++i) {
