@@ -113,3 +113,19 @@ def test_circuit_without_gates_or_rotations():
     E, g = AdjointEngine(n, f32=True, method="jit").energy_and_grad(pc, [0.1, 0.2, 0.3], a, b)
     assert abs(E - O.energy(O.simulate(qc), a, b)) <= 1e-5
     assert np.all(g == 0.0) and g.size == 3
+
+
+@pytest.mark.parametrize("knobs", [{"jit_lr": 6}, {"m": 12, "k": 2}])
+def test_plan_knobs_keep_the_gradient(knobs):
+    # other register-bit counts and staging of the two programs: the same gradient
+    from frontierlabproject_b200.adjoint import AdjointEngine, ParamCircuit
+    n, L = 14, 3
+    rng = np.random.default_rng(4)
+    th = rng.uniform(-np.pi, np.pi, 2 * n * L)
+    a, b = C.hea_observable(n, 5)
+    E_ref, g_ref = O.adjoint_gradient(C.hea_ansatz(n, L, th), a, b)
+    eng = AdjointEngine(n, f32=True, method="jit")
+    eng.set_config(**knobs)
+    E, g = eng.energy_and_grad(ParamCircuit.hea(n, L), th, a, b)
+    assert abs(E - E_ref) <= 1e-5 * max(1.0, abs(E_ref))
+    assert _rel(g, g_ref) <= 1e-5
