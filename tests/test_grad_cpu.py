@@ -125,3 +125,37 @@ def test_reverse_program_kernels_compile_without_spills(native_lib):
     for line in text.splitlines():
         if "spill stores" in line:
             assert int(line.split("bytes spill stores")[0].split(",")[-1].strip()) == 0, line
+
+
+def test_gradient_entry_points_validate_ops(native_lib):
+    import ctypes
+    from frontierlabproject_b200 import _native as N
+    from frontierlabproject_b200.adjoint import AdjOps
+    n = 10
+    pc = ParamCircuit(n, [ParamGate("ry", (0,), 0), ParamGate("cz", (0, 1))], 1)
+    tab = AdjOps(pc)  # owns the matrices the op table points to
+    ops = tab.update([0.3])
+    z = np.zeros(1 << n, np.complex64)
+    g = np.zeros(1)
+
+    def emulate(o, nq=n, npar=1):
+        return N.lib().qs_grad_emulate(nq, o.ctypes.data, len(o), npar, None, z.ctypes.data, z.ctypes.data,
+                                       g.ctypes.data)
+
+    assert emulate(ops) == 0
+    bad = ops.copy()
+    bad[0]["q0"] = n
+    assert emulate(bad) == N.QS_ERR_INVALID and b"invalid q0" in N.lib().qs_last_error()
+    bad = ops.copy()
+    bad[0]["grad_index"] = 1
+    assert emulate(bad) == N.QS_ERR_INVALID and b"grad_index" in N.lib().qs_last_error()
+    bad = ops.copy()
+    bad[1]["gen"] = 3
+    assert emulate(bad) == N.QS_ERR_INVALID and b"two-qubit" in N.lib().qs_last_error()
+    bad = ops.copy()
+    bad[1]["q1"] = 0
+    assert emulate(bad) == N.QS_ERR_INVALID and b"q0/q1" in N.lib().qs_last_error()
+    assert emulate(ops, nq=9) == N.QS_ERR_INVALID
+    h = ctypes.c_void_p()
+    assert N.lib().qs_grad_create(9, ops.ctypes.data, len(ops), 1, None, ctypes.byref(h)) == N.QS_ERR_INVALID
+    assert not h.value
