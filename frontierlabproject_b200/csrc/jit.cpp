@@ -893,9 +893,45 @@ std::string jit_source(const Program& prog, int pass_begin, int pass_end, uint64
         gen_term(G, gis[k], prog.grad_gen[k], prog.grad_term[k] - t0, A, &pending);
         if ((int)pending.size() >= kTermBatch) gen_term_flush(G, &pending, std::max(1, nt));
       };
+      // Z rotations on fixed bits: their terms are taken at the phase start (the registers are
+      // untouched yet; Z of a fixed bit commutes with the phase) and all share the thread's sum
+      // gb_ = sum_i Im(conj(lam_i) psi_i), signed by the bit.  For a bit that is uniform over the
+      // warp (a group or warp-index bit) one warp sum gw_ of gb_ serves every such term.
+      const int ntr = std::max(1, nt);
+      bool have_base = false, have_wsum = false;
+      auto fixed_z_term = [&](int gi) {
+        const int k = ph.gate0 + gi;
+        if (!grad || !prog.grad_gen[k]) return;
+        const GateInstr& g = gis[k];
+        if (prog.grad_gen[k] != 3) throw std::runtime_error("jit: an X or Y rotation on a fixed bit");
+        if (A < 0) throw std::runtime_error("jit: the lam bit is not a register bit");
+        const int P = g.a - kFixed, local = prog.grad_term[k] - t0;
+        if (!have_base) {
+          G.o << "float gb_=0.f;\n#pragma unroll\nfor(int i=0;i<NR;++i) if(!(i&" << (1 << A)
+              << ")){const float2 p=a[i],l=a[i|" << (1 << A) << "];gb_+=l.x*p.y-l.y*p.x;}\n";
+          have_base = true;
+        }
+        bool uniform = true;
+        for (int j = 0; j < 5 && j < pd.m - pd.r; ++j)
+          if (pd.sbit[ph.tbit[j]] == P) uniform = false;
+        if (uniform) {
+          if (!have_wsum) {
+            G.o << "float gw_=gb_;gw_+=__shfl_xor_sync(0xffffffffu,gw_,16);gw_+=__shfl_xor_sync(0xffffffffu,gw_,8);"
+                << "gw_+=__shfl_xor_sync(0xffffffffu,gw_,4);gw_+=__shfl_xor_sync(0xffffffffu,gw_,2);"
+                << "gw_+=__shfl_xor_sync(0xffffffffu,gw_,1);\n";
+            have_wsum = true;
+          }
+          G.o << "if((threadIdx.x&31u)==0u)ga[(threadIdx.x>>5)*" << ntr << "+" << local << "]+=(double)("
+              << bitcond(P) << "?-gw_:gw_);\n";
+        } else {
+          G.o << "float gt" << local << "=" << bitcond(P) << "?-gb_:gb_;\n";
+          pending.push_back(local);
+          if ((int)pending.size() >= kTermBatch) gen_term_flush(G, &pending, ntr);
+        }
+      };
       for (int gi = 0; gi < ph.ngate; ++gi)
         if (fixed_diag(gis[ph.gate0 + gi])) {
-          term(gi);  // the phase's registers are untouched yet: Z of a fixed bit commutes with the phase
+          fixed_z_term(gi);
           gen_gate(G, gis[ph.gate0 + gi], pd, ph);
         }
       int absorber = -1;
